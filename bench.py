@@ -1,0 +1,352 @@
+"""Benchmark of the B200 Q2-P1disc Stokes operator (pTatin3D hot path).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload c2|c1|c0] [--no-cpu-baseline]
+
+One step = one FP64 A11 apply (MatMult_MFStokes_A11: Dirichlet columns zeroed,
+rows copied) over the whole 128^3 Q2 box of the precision workload (257^3
+nodes, 50.9M velocity dofs; nodes perturbed +-0.05h; three viscosity layers
+1e3/1/1e-1 plus 64 inclusions 1e-3..1e3; free-slip box BCs).  Inputs are
+resident in HBM and larger than L2 (u, y 407 MB each; eta 453 MB), so no L2
+flush is needed between steps.
+
+value     = 3N / t_apply in GDoF/s, the device-timed apply (CUDA events on the
+            op's stream), whole job over all ranks (replicas: each rank runs
+            the same problem; the operator is single-GPU by design).
+e2e       = the same metric through the public host-pointer API
+            (pt_matmult_a11_h): pinned host x -> device, apply, device -> host y.
+roofline  = algorithmic bytes of one apply / its device time against the
+            measured HBM copy bandwidth (MEASURED_PEAKS.json).
+cpu_baseline = the reference's own AVX A11 (oracle/_ref, compiled from the
+            reference sources) on a 128x128x16 slab of the same workload,
+            on all host cores.
+--impl reference times that reference CPU path only and prints its line.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(REPO, "ptatin-gene_b200"))
+
+METRIC = "Q2 A11 GDoF/s FP64 vs FP32 @128³; batched solves/s & p99 @rtol 1e-8"
+UNIT = "GDoF/s"
+
+
+def algorithmic_bytes(m, s=8):
+    """u + coords + y (3N each) + eta (27 nel), s bytes per value."""
+    return (9 * m.nnodes + 27 * m.nel) * s
+
+
+def load_peaks():
+    p = os.path.join(REPO, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index=0):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self._t = threading.Thread(target=self._read, daemon=True)
+            self._t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_setup(args):
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if ws > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+        pg = dist
+    return ws, rank, local, pg
+
+
+def max_over_ranks(x, pg, device):
+    if pg is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(pg, device):
+    if pg is not None:
+        import torch
+        t = torch.zeros(1, device=device)
+        pg.all_reduce(t)
+    import torch
+    torch.cuda.synchronize()
+
+
+def cpu_reference_sample(workload_slab=("c2", 16), seconds=12.0, kind="avx"):
+    """Time the reference's own A11 (oracle/_ref) on a z-slab of the workload."""
+    import oracle
+    from pt_b200 import mesh as M
+    if not oracle.RefCPU.available():
+        oracle.build()
+    r = oracle.RefCPU()
+    mz = workload_slab[1]
+    m = M.make_mesh(128, 128, mz, perturb=0.05, seed=0)
+    eta = M.eta_layered(m, seed=1)
+    mask = M.bc_mask_freeslip(*m.dims)
+    x = M.uniform_vec(m.nvel, 7)
+    x[mask.astype(bool)] = 0.0
+    r.a11(m.dims, m.coords, eta, x, kind)  # warm-up
+    times = []
+    t_end = time.perf_counter() + seconds
+    while time.perf_counter() < t_end or len(times) < 2:
+        t0 = time.perf_counter()
+        r.a11(m.dims, m.coords, eta, x, kind)
+        times.append(time.perf_counter() - t0)
+    best = min(times)
+    return {
+        "value": m.nvel / best / 1e9,
+        "unit": UNIT,
+        "cores": os.cpu_count(),
+        "kind": "reference",
+        "sample": f"reference {kind} A11 (MFStokesWrapper_A11_AVX, OpenMP {os.cpu_count()} threads) on a "
+                  f"128x128x{mz} slab of the 128^3 workload, best of {len(times)} applies",
+        "seconds_per_apply": best,
+    }
+
+
+def run_reference(args):
+    ws, rank, local, pg = int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), 0, None
+    if rank != 0:
+        return 0
+    try:
+        import oracle
+        if not oracle.RefCPU.available():
+            oracle.build()
+        oracle.RefCPU()
+    except Exception as e:  # pragma: no cover
+        print(json.dumps({"impl": "reference", "unavailable": f"reference CPU build missing: {e}"}))
+        return 0
+    from pt_b200 import mesh as M
+    r = oracle.RefCPU()
+    mz = 16
+    m = M.make_mesh(128, 128, mz, perturb=0.05, seed=0)
+    eta = M.eta_layered(m, seed=1)
+    mask = M.bc_mask_freeslip(*m.dims)
+    x = M.uniform_vec(m.nvel, 7)
+    x[mask.astype(bool)] = 0.0
+    for _ in range(args.warmup):
+        r.a11(m.dims, m.coords, eta, x, "avx")
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        r.a11(m.dims, m.coords, eta, x, "avx")
+    dt = (time.perf_counter() - t0) / args.steps
+    v = m.nvel / dt / 1e9
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "A11 FP64 apply, 128x128x16 slab of the 128^3 Q2 box (perturbed +-0.05h, layered "
+                               "eta 1e6 contrast), reference CPU (oracle/_ref, avx)",
+                   "global_batch": 1, "seq_len": 0, "parallelism": "cpu-openmp"},
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
+                         "sample": "128x128x16 slab, MFStokesWrapper_A11_AVX compiled from the reference sources"},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def run_ours(args):
+    import torch
+
+    from pt_b200 import MatStokesMF
+    from pt_b200 import mesh as M
+
+    ws, rank, local, pg = dist_setup(args)
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+
+    m, eta, mask = M.problem(args.workload, seed=0)
+    stream = torch.cuda.Stream(device=dev)
+    op = MatStokesMF(*m.dims, a11_op=args.a11_op, stream=stream)
+    op.SetUp(m.coords, eta, mask)
+    x = torch.from_numpy(M.uniform_vec(m.nvel, 7)).to(dev)
+    y = torch.empty_like(x)
+    x32, y32 = x.float(), torch.empty(m.nvel, dtype=torch.float32, device=dev)
+    p = torch.from_numpy(M.uniform_vec(m.npres, 8)).to(dev)
+    yp = torch.empty(m.npres, dtype=torch.float64, device=dev)
+    torch.cuda.synchronize()
+
+    def timed(fn, k):
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            ev0.record(stream)
+            for _ in range(k):
+                fn()
+            ev1.record(stream)
+        ev1.synchronize()
+        return ev0.elapsed_time(ev1) / 1e3
+
+    # ---- headline: FP64 A11 (MatShell level), device resident ----------------
+    for _ in range(max(args.warmup, 3)):
+        op.MatMult_MFStokes_A11(x, y)
+    barrier(pg, dev)
+    op.reset_launch_count()
+    with ClockSampler(local) as clk:
+        t = timed(lambda: op.MatMult_MFStokes_A11(x, y), args.steps)
+    launches = op.launch_count()
+    t = max_over_ranks(t, pg, dev)
+    t_apply = t / args.steps
+    value = ws * m.nvel / t_apply / 1e9
+
+    # ---- roofline of the A11 apply ---------------------------------------------
+    peak, peak_kind = load_peaks()
+    bytes_alg = algorithmic_bytes(m)
+    achieved = bytes_alg / t_apply / 1e9
+
+    # ---- other operators and FP32 (device resident) ------------------------------
+    extra = {}
+    if not args.quick:
+        def rate(fn, n):
+            for _ in range(2):
+                fn()
+            dt = timed(fn, max(2, args.steps // 2)) / max(2, args.steps // 2)
+            return n / dt / 1e9, dt * 1e3
+        extra["a11_fp32_gdofs"], extra["a11_fp32_ms"] = rate(lambda: op.MatMult_MFStokes_A11(x32, y32), m.nvel)
+        extra["diag_gdofs"], extra["diag_ms"] = rate(lambda: op.MatGetDiagonal_MFStokes_A11(y), m.nvel)
+        extra["a21_gdofs"], extra["a21_ms"] = rate(lambda: op.MatMult_MFStokes_A21(x, yp), m.nvel)
+        extra["a12_gdofs"], extra["a12_ms"] = rate(lambda: op.MatMult_MFStokes_A12(p, y), m.nvel)
+        extra["a11_flops_per_element_ref_count"] = 17253
+
+    # ---- e2e through the host-pointer API (pinned buffers) ----------------------------
+    xh = torch.empty(m.nvel, dtype=torch.float64, pin_memory=True)
+    xh.copy_(x.cpu())
+    yh = torch.empty(m.nvel, dtype=torch.float64, pin_memory=True)
+    xn, yn = xh.numpy(), yh.numpy()
+    op.MatMult_MFStokes_A11(xn, yn)
+    k_e2e = max(2, min(args.steps, 5))
+    barrier(pg, dev)
+    t0 = time.perf_counter()
+    for _ in range(k_e2e):
+        op.MatMult_MFStokes_A11(xn, yn)
+    t_e2e = max_over_ranks((time.perf_counter() - t0) / k_e2e, pg, dev)
+    e2e = {"value": ws * m.nvel / t_e2e / 1e9, "unit": UNIT, "h2d_bytes_per_step": 8 * m.nvel,
+           "d2h_bytes_per_step": 8 * m.nvel, "ms_per_step": t_e2e * 1e3,
+           "path": "pt_matmult_a11_h (MatMult_MFStokes_A11 on pinned numpy arrays)"}
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        try:
+            cpu = cpu_reference_sample(seconds=args.cpu_seconds)
+        except Exception as e:  # pragma: no cover
+            cpu = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
+                   "sample": f"unavailable: {e}"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+            "warmup": max(args.warmup, 3), "ms_per_step": t_apply * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"A11 FP64 MatMult, {m.mx}x{m.my}x{m.mz} Q2 box ({m.nvel} velocity dofs), "
+                                   f"perturbed +-0.05h, layered eta + 64 inclusions (1e6 contrast), free-slip BCs",
+                       "global_batch": 1, "seq_len": 0, "parallelism": f"replicas{ws}",
+                       "a11_op": op.a11_op, "l2": "inputs larger than L2 (no flush)"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind,
+                         "algorithmic_bytes_per_apply": bytes_alg},
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "gpu_launches": launches,
+            "clocks": clk.summary(),
+            "extra": extra,
+        }
+        print(json.dumps(line))
+    op.Destroy()
+    if pg is not None:
+        pg.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="c2")
+    ap.add_argument("--a11-op", default="b200")
+    ap.add_argument("--quick", action="store_true", help="headline A11 only")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

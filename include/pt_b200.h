@@ -1,0 +1,154 @@
+/*
+ * pt_b200.h -- C ABI of libpt_b200.so, the B200 (sm_100a) implementation of
+ * pTatin3D's matrix-free Q2-P1disc Stokes operator hot path.
+ *
+ * Plain C types only (no CUDA or PETSc types): pointers, sizes, a status code.
+ * Streams are passed as `void *` holding a cudaStream_t (NULL = the op's own
+ * stream).  Every entry point returns pt_status and never exits the process
+ * (the reference CUDA back-end calls cudaDeviceReset()+exit on errors,
+ * src/stokes_operators_cuda.cu:46-57).
+ *
+ * One rank's local problem: on one rank the DMDA ghosted local numbering
+ * equals the global numbering, so vectors are the reference's local arrays:
+ *   velocity  [3*N]   interleaved (u,v,w) per node, node id i + j*X + k*X*Y,
+ *                     X = 2*mx+1, Y = 2*my+1   (src/ptatin3d_stokes.c:121-146)
+ *   pressure  [4*nel] four P1 dofs per element (element e = ei+ej*mx+ek*mx*my)
+ *   coords    [3*N]   like velocity
+ *   eta       [27*nel] quadrature-point viscosity, element-major, qp index
+ *                     a*9+b*3+c (c along xi) -- the QPntVolCoefStokes.eta order
+ *                     (include/QPntVolCoefStokes_def.h:41-46)
+ *   mask      [3*N]   uint8, nonzero on Dirichlet dofs (BCList, scale 1)
+ *
+ * Two levels of entry point:
+ *  - "SpMVOp" level (pt_a11_apply_*, pt_a11_diag_*, pt_a12_apply_*,
+ *    pt_a21_apply_*): the element-loop kernels the reference dispatches
+ *    through MatA11MF->SpMVOp_MatMult (include/stokes_operators.h:61), i.e.
+ *    MFStokesWrapper_A11_{Tensor,AVX,CUDA}, MFStokesWrapper_diagA11,
+ *    MFStokesWrapper_A12(_AVX), MFStokesWrapper_A21.  Input already has
+ *    Dirichlet entries zeroed by the caller; output is the unassembled local
+ *    sum with no BC row treatment.  Output is overwritten (the reference
+ *    caller zeroes Yu first, src/stokes_operators.c:1195-1196, so overwrite
+ *    and accumulate agree).
+ *  - "MatShell" level (pt_matmult_*, pt_getdiag_*): the BC semantics of
+ *    MatMult_MFStokes_A11 / MatGetDiagonal_MFStokes_A11 / MatMult_MFStokes_A12 /
+ *    MatMult_MFStokes_A21 (src/stokes_operators.c:1156-1222, 1072-1113,
+ *    1301-1370, 1444-1509) for one rank, using the mask set with
+ *    pt_op_set_bc_mask.
+ *
+ * Suffixes: _h = host pointers (the call copies in, computes, copies out and
+ * synchronises); _d = device pointers, asynchronous on the op's stream.
+ */
+#ifndef PT_B200_H
+#define PT_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  PT_OK = 0,
+  PT_ERR_BAD_ARG = 1,    /* invalid size, NULL pointer, unknown name */
+  PT_ERR_OOM = 2,        /* device allocation failed */
+  PT_ERR_CUDA = 3,       /* a CUDA runtime call failed; see pt_last_error() */
+  PT_ERR_TIMEOUT = 4,    /* a bounded device-side wait gave up */
+  PT_ERR_STATE = 5,      /* coords / eta / mask not set before an apply */
+  PT_ERR_UNSUPPORTED = 6 /* valid request this build does not implement */
+} pt_status;
+
+typedef struct {
+  int32_t mx, my, mz; /* Q2 elements per axis (>= 1 each) */
+} pt_mesh_desc;
+
+typedef struct pt_op pt_op;
+
+/* Human-readable text of the last error on this thread ("" if none). */
+const char *pt_last_error(void);
+/* Library version string. */
+const char *pt_version(void);
+
+/* Operator context.  Replaces MatA11MFCreate/MatA11MFSetup + the back-end
+ * SpMVOp_SetUp (src/stokes_operators.c:104-160, 230-279;
+ * src/stokes_operators_cuda.cu:243-323).  Allocates device storage for the
+ * mesh data; vectors passed to _h calls are staged through op-owned buffers. */
+pt_status pt_op_create(const pt_mesh_desc *desc, pt_op **op);
+/* Replaces SpMVOp_Destroy (MFA11Destroy_CUDA, src/stokes_operators_cuda.cu:300-323). */
+pt_status pt_op_destroy(pt_op *op);
+/* Stream for all subsequent work of this op (cudaStream_t as void*). */
+pt_status pt_op_set_stream(pt_op *op, void *stream);
+pt_status pt_op_get_sizes(const pt_op *op, int64_t *nvel, int64_t *npres, int64_t *nel);
+
+/* Mesh data.  Replaces the coordinate / QPntVolCoefStokes uploads of
+ * CopyTo_A11_CUDA (src/stokes_operators_cuda.cu:325-431), done here once per
+ * change of the data (the reference re-uploads on PetscObjectState change). */
+pt_status pt_op_set_coords_h(pt_op *op, const double *coords);
+pt_status pt_op_set_coords_d(pt_op *op, const double *coords);
+pt_status pt_op_set_eta_h(pt_op *op, const double *eta);
+pt_status pt_op_set_eta_d(pt_op *op, const double *eta);
+pt_status pt_op_set_bc_mask_h(pt_op *op, const uint8_t *mask); /* NULL = no Dirichlet dofs */
+
+/* ---- SpMVOp level ------------------------------------------------------ */
+
+/* y = A11 u (unassembled local).  Replaces MFStokesWrapper_A11_{Tensor,AVX,CUDA}
+ * (src/stokes_operators_tensor.c:181-286, src/stokes_operators_avx.c:206-312,
+ * src/stokes_operators_cuda.cu:457-532). */
+pt_status pt_a11_apply_h(pt_op *op, const double *u, double *y);
+pt_status pt_a11_apply_d(pt_op *op, const double *u, double *y);
+/* Single-precision apply (FP32 arithmetic and accumulation) for smoothers. */
+pt_status pt_a11_apply_f32_d(pt_op *op, const float *u, float *y);
+
+/* d = diag(A11) (unassembled local).  Replaces MFStokesWrapper_diagA11
+ * (src/stokes_operators_mf.c:71-135). */
+pt_status pt_a11_diag_h(pt_op *op, double *d);
+pt_status pt_a11_diag_d(pt_op *op, double *d);
+
+/* yp = B u (divergence, A21).  Replaces MFStokesWrapper_A21
+ * (src/stokes_operators_mf.c:862-937). */
+pt_status pt_a21_apply_h(pt_op *op, const double *u, double *yp);
+pt_status pt_a21_apply_d(pt_op *op, const double *u, double *yp);
+
+/* yu = B^T p (gradient, A12).  Replaces MFStokesWrapper_A12_AVX / MFStokesWrapper_A12
+ * (src/stokes_operators_avx.c:682-829, src/stokes_operators_mf.c:792-860). */
+pt_status pt_a12_apply_h(pt_op *op, const double *p, double *yu);
+pt_status pt_a12_apply_d(pt_op *op, const double *p, double *yu);
+
+/* ---- MatShell level (BC semantics, one rank) -------------------------- */
+
+/* y = A11 x with Dirichlet columns zeroed and rows y_k = x_k
+ * (MatMult_MFStokes_A11, src/stokes_operators.c:1156-1222). */
+pt_status pt_matmult_a11_h(pt_op *op, const double *x, double *y);
+pt_status pt_matmult_a11_d(pt_op *op, const double *x, double *y);
+pt_status pt_matmult_a11_f32_d(pt_op *op, const float *x, float *y);
+/* diag(A11) with Dirichlet slots set to 1 (MatGetDiagonal_MFStokes_A11,
+ * src/stokes_operators.c:1072-1113). */
+pt_status pt_getdiag_a11_h(pt_op *op, double *d);
+pt_status pt_getdiag_a11_d(pt_op *op, double *d);
+/* yu = B^T p with Dirichlet rows zeroed (MatMult_MFStokes_A12,
+ * src/stokes_operators.c:1301-1370). */
+pt_status pt_matmult_a12_h(pt_op *op, const double *p, double *yu);
+pt_status pt_matmult_a12_d(pt_op *op, const double *p, double *yu);
+/* yp = B u with Dirichlet columns of u zeroed (MatMult_MFStokes_A21,
+ * src/stokes_operators.c:1444-1509). */
+pt_status pt_matmult_a21_h(pt_op *op, const double *u, double *yp);
+pt_status pt_matmult_a21_d(pt_op *op, const double *u, double *yp);
+
+/* ---- selection, in the style of -a11_op --------------------------------- */
+
+/* Select the A11 kernel by name, like the reference's -a11_op function list
+ * (src/stokes_operators.c:123-154).  Names: "b200" (default, the tuned
+ * kernel) and "b200_colour" (8-colour element kernel).  Unknown names give
+ * PT_ERR_BAD_ARG, as the reference's SETERRQ1 "No -a11_op %s". */
+pt_status pt_op_set_a11_kernel(pt_op *op, const char *name);
+const char *pt_op_get_a11_kernel(const pt_op *op);
+
+/* Device-side timing helpers: launch count of this library's kernels on this
+ * op since the last reset (for benchmark accounting). */
+int64_t pt_op_launch_count(const pt_op *op);
+void pt_op_reset_launch_count(pt_op *op);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

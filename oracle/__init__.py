@@ -1,0 +1,209 @@
+"""CPU oracle for the Q2-P1disc matrix-free Stokes operator.
+
+TEST INFRASTRUCTURE ONLY.  Only ``tests/``, ``__graft_entry__.smoke()`` and the
+CPU-baseline leg of ``bench.py`` may import this package, and only as the
+checker (or the timed CPU reference arm), never as the thing measured or
+shipped.  The product path (``ptatin-gene_b200``) never imports it.
+
+Two checkers live here:
+
+* ``Oracle``   -- ``liboracle.so``, a plain-C restatement of the reference's
+  CPU arithmetic (``pt_oracle.c``; each routine cites the reference file:line
+  it restates).
+* ``RefCPU``   -- ``_ref/libptref.so``, the reference's own
+  ``stokes_operators_{tensor,avx,mf}.c`` and ``element_utils_q{1,2}.c``
+  compiled unmodified against the PETSc stand-in headers in ``ref_stub/``
+  (``ref_glue.c`` only marshals arrays).  Present where the reference tree was
+  available at build time.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_ORA_SO = os.path.join(_HERE, "liboracle.so")
+_REF_SO = os.path.join(_HERE, "_ref", "libptref.so")
+
+_dp = ctypes.POINTER(ctypes.c_double)
+_u8p = ctypes.POINTER(ctypes.c_uint8)
+_i32p = ctypes.POINTER(ctypes.c_int32)
+
+
+def build(quiet: bool = True) -> None:
+    """Compile liboracle.so (and _ref/libptref.so where the reference exists)."""
+    out = subprocess.run(["make", "-C", _HERE, "all"], capture_output=True, text=True)
+    if out.returncode != 0:
+        raise RuntimeError("oracle build failed:\n" + out.stdout + out.stderr)
+    if not quiet:
+        print(out.stdout)
+
+
+def _ptr(a, t=_dp):
+    return a.ctypes.data_as(t)
+
+
+def _f64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def _mask(a):
+    return np.ascontiguousarray(a, dtype=np.uint8)
+
+
+class Oracle:
+    """ctypes front-end of liboracle.so (Route B restatement)."""
+
+    def __init__(self, path: str = _ORA_SO):
+        if not os.path.exists(path):
+            build()
+        self.lib = ctypes.CDLL(path)
+        L = self.lib
+        i = ctypes.c_int
+        for name in ("ora_a11_tensor", "ora_a11_ref"):
+            getattr(L, name).argtypes = [i, i, i, _dp, _dp, _dp, _dp]
+        L.ora_a11_diag.argtypes = [i, i, i, _dp, _dp, _dp]
+        for name in ("ora_a21_ref", "ora_a12_ref", "ora_a12_tensor"):
+            getattr(L, name).argtypes = [i, i, i, _dp, _dp, _dp]
+        L.ora_elements_q2.argtypes = [i, i, i, _i32p]
+        L.ora_gauss3.argtypes = [_dp, _dp]
+        L.ora_matmult_a11.argtypes = [i, i, i, _dp, _dp, _u8p, _dp, _dp, i]
+        L.ora_getdiag_a11.argtypes = [i, i, i, _dp, _dp, _u8p, _dp]
+        L.ora_matmult_a12.argtypes = [i, i, i, _dp, _u8p, _dp, _dp, i]
+        L.ora_matmult_a21.argtypes = [i, i, i, _dp, _u8p, _dp, _dp]
+        L.ora_a11_flops.argtypes = [ctypes.c_int64]
+        L.ora_a11_flops.restype = ctypes.c_double
+        L.ora_num_threads.restype = ctypes.c_int
+
+    # element-loop kernels (y = 0 + contributions, unassembled semantics)
+    def a11(self, dims, coords, eta, u, variant="tensor"):
+        mx, my, mz = dims
+        y = np.zeros_like(_f64(u))
+        fn = self.lib.ora_a11_tensor if variant == "tensor" else self.lib.ora_a11_ref
+        fn(mx, my, mz, _ptr(_f64(coords)), _ptr(_f64(eta)), _ptr(_f64(u)), _ptr(y))
+        return y
+
+    def diag(self, dims, coords, eta):
+        mx, my, mz = dims
+        y = np.zeros(3 * (2 * mx + 1) * (2 * my + 1) * (2 * mz + 1))
+        self.lib.ora_a11_diag(mx, my, mz, _ptr(_f64(coords)), _ptr(_f64(eta)), _ptr(y))
+        return y
+
+    def a21(self, dims, coords, u):
+        mx, my, mz = dims
+        y = np.zeros(4 * mx * my * mz)
+        self.lib.ora_a21_ref(mx, my, mz, _ptr(_f64(coords)), _ptr(_f64(u)), _ptr(y))
+        return y
+
+    def a12(self, dims, coords, p, variant="tensor"):
+        mx, my, mz = dims
+        y = np.zeros(3 * (2 * mx + 1) * (2 * my + 1) * (2 * mz + 1))
+        fn = self.lib.ora_a12_tensor if variant == "tensor" else self.lib.ora_a12_ref
+        fn(mx, my, mz, _ptr(_f64(coords)), _ptr(_f64(p)), _ptr(y))
+        return y
+
+    # MatShell-level operators (BC semantics of stokes_operators.c)
+    def matmult_a11(self, dims, coords, eta, mask, x, variant="tensor"):
+        mx, my, mz = dims
+        y = np.zeros_like(_f64(x))
+        self.lib.ora_matmult_a11(mx, my, mz, _ptr(_f64(coords)), _ptr(_f64(eta)),
+                                 _ptr(_mask(mask), _u8p), _ptr(_f64(x)), _ptr(y),
+                                 0 if variant == "tensor" else 1)
+        return y
+
+    def getdiag_a11(self, dims, coords, eta, mask):
+        mx, my, mz = dims
+        y = np.zeros(len(mask))
+        self.lib.ora_getdiag_a11(mx, my, mz, _ptr(_f64(coords)), _ptr(_f64(eta)),
+                                 _ptr(_mask(mask), _u8p), _ptr(y))
+        return y
+
+    def matmult_a12(self, dims, coords, mask, p, variant="tensor"):
+        mx, my, mz = dims
+        y = np.zeros(len(mask))
+        self.lib.ora_matmult_a12(mx, my, mz, _ptr(_f64(coords)), _ptr(_mask(mask), _u8p),
+                                 _ptr(_f64(p)), _ptr(y), 0 if variant == "tensor" else 1)
+        return y
+
+    def matmult_a21(self, dims, coords, mask, u):
+        mx, my, mz = dims
+        y = np.zeros(4 * mx * my * mz)
+        self.lib.ora_matmult_a21(mx, my, mz, _ptr(_f64(coords)), _ptr(_mask(mask), _u8p),
+                                 _ptr(_f64(u)), _ptr(y))
+        return y
+
+    def elements(self, dims):
+        mx, my, mz = dims
+        e = np.zeros(27 * mx * my * mz, dtype=np.int32)
+        self.lib.ora_elements_q2(mx, my, mz, _ptr(e, _i32p))
+        return e.reshape(-1, 27)
+
+    def gauss3(self):
+        x = np.zeros(3)
+        w = np.zeros(3)
+        self.lib.ora_gauss3(_ptr(x), _ptr(w))
+        return x, w
+
+    def a11_flops(self, nel):
+        return self.lib.ora_a11_flops(nel)
+
+    def num_threads(self):
+        return self.lib.ora_num_threads()
+
+
+class RefCPU:
+    """ctypes front-end of _ref/libptref.so (the reference's own sources)."""
+
+    KINDS = {"tensor": 0, "avx": 1, "ref": 2}
+
+    def __init__(self, path: str = _REF_SO):
+        if not os.path.exists(path):
+            raise FileNotFoundError(path)
+        self.lib = ctypes.CDLL(path)
+        L = self.lib
+        i = ctypes.c_int
+        L.ref_a11.argtypes = [i, i, i, i, _dp, _dp, _dp, _dp]
+        L.ref_diag.argtypes = [i, i, i, _dp, _dp, _dp]
+        L.ref_a21.argtypes = [i, i, i, _dp, _dp, _dp]
+        L.ref_a12.argtypes = [i, i, i, i, _dp, _dp, _dp]
+        L.ref_has_avx.restype = i
+
+    @staticmethod
+    def available() -> bool:
+        return os.path.exists(_REF_SO)
+
+    def _check(self, rc, what):
+        if rc != 0:
+            raise RuntimeError(f"reference {what} returned PetscErrorCode {rc}")
+
+    def a11(self, dims, coords, eta, u, kind="tensor"):
+        mx, my, mz = dims
+        u = _f64(u).copy()
+        y = np.zeros_like(u)
+        self._check(self.lib.ref_a11(self.KINDS[kind], mx, my, mz, _ptr(_f64(coords)),
+                                     _ptr(_f64(eta)), _ptr(u), _ptr(y)), "A11")
+        return y
+
+    def diag(self, dims, coords, eta):
+        mx, my, mz = dims
+        y = np.zeros(3 * (2 * mx + 1) * (2 * my + 1) * (2 * mz + 1))
+        self._check(self.lib.ref_diag(mx, my, mz, _ptr(_f64(coords)), _ptr(_f64(eta)), _ptr(y)), "diag")
+        return y
+
+    def a21(self, dims, coords, u):
+        mx, my, mz = dims
+        u = _f64(u).copy()
+        y = np.zeros(4 * mx * my * mz)
+        self._check(self.lib.ref_a21(mx, my, mz, _ptr(_f64(coords)), _ptr(u), _ptr(y)), "A21")
+        return y
+
+    def a12(self, dims, coords, p, kind="avx"):
+        mx, my, mz = dims
+        p = _f64(p).copy()
+        y = np.zeros(3 * (2 * mx + 1) * (2 * my + 1) * (2 * mz + 1))
+        self._check(self.lib.ref_a12(self.KINDS[kind], mx, my, mz, _ptr(_f64(coords)),
+                                     _ptr(p), _ptr(y)), "A12")
+        return y

@@ -1,0 +1,562 @@
+// C ABI of libpt_b200.so (declared in include/pt_b200.h).
+//
+// The op owns device copies of the mesh data (coordinates, quadrature-point
+// viscosity, Dirichlet mask), FP32 shadows of coordinates/viscosity for the
+// single-precision apply, and staging vectors for the host-pointer calls.
+// Kernels live in kernels_*.cuh; this file does argument checking, memory,
+// streams and the BC fix-ups of the MatShell-level calls.
+#include <cuda_runtime.h>
+
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+
+#include "pt_b200.h"
+#include "kernels_colour.cuh"
+
+namespace {
+
+thread_local std::string g_err;
+
+pt_status fail(pt_status s, const char *fmt, ...)
+{
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  g_err = buf;
+  return s;
+}
+
+#define PT_CUDA(call)                                                                              \
+  do {                                                                                             \
+    cudaError_t _e = (call);                                                                       \
+    if (_e != cudaSuccess)                                                                         \
+      return fail(_e == cudaErrorMemoryAllocation ? PT_ERR_OOM : PT_ERR_CUDA, "%s: %s (%s:%d)",    \
+                  #call, cudaGetErrorString(_e), __FILE__, __LINE__);                              \
+  } while (0)
+
+#define PT_LAUNCHED(op)                                                                            \
+  do {                                                                                             \
+    (op)->launches++;                                                                              \
+    cudaError_t _e = cudaGetLastError();                                                           \
+    if (_e != cudaSuccess)                                                                         \
+      return fail(PT_ERR_CUDA, "kernel launch: %s (%s:%d)", cudaGetErrorString(_e), __FILE__,     \
+                  __LINE__);                                                                       \
+  } while (0)
+
+enum A11Kernel { A11_STREAM = 0, A11_COLOUR = 1 };
+
+}  // namespace
+
+struct pt_op {
+  int mx, my, mz;
+  int64_t nnodes, nvel, nel, npres;
+  cudaStream_t stream;
+  bool own_stream;
+  double *d_coords, *d_eta;
+  float *d_coords32, *d_eta32;
+  uint8_t *d_mask;
+  bool has_coords, has_eta, has_mask;
+  double *d_u, *d_y, *d_p; // staging for _h calls
+  int a11_kernel;
+  int64_t launches;
+  int device;
+};
+
+namespace {
+
+constexpr int TPB = 128;
+
+inline unsigned nblocks(int64_t n, int tpb = TPB) { return (unsigned)((n + tpb - 1) / tpb); }
+
+__global__ void to_f32_kernel(const double *__restrict__ a, float *__restrict__ b, int64_t n)
+{
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    b[i] = (float)a[i];
+}
+
+template <typename T>
+__global__ void bc_copy_kernel(const uint8_t *__restrict__ mask, const T *__restrict__ x, T *__restrict__ y, int64_t n)
+{
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    if (mask[i]) y[i] = x[i];
+}
+
+__global__ void bc_value_kernel(const uint8_t *__restrict__ mask, double v, double *__restrict__ y, int64_t n)
+{
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    if (mask[i]) y[i] = v;
+}
+
+unsigned grid_stride_blocks(int64_t n)
+{
+  const int64_t b = (n + 255) / 256;
+  return (unsigned)(b < 148 * 16 ? (b < 1 ? 1 : b) : 148 * 16);
+}
+
+pt_status check_ready(const pt_op *op, bool need_eta)
+{
+  if (!op) return fail(PT_ERR_BAD_ARG, "op is NULL");
+  if (!op->has_coords) return fail(PT_ERR_STATE, "coordinates not set (pt_op_set_coords_*)");
+  if (need_eta && !op->has_eta) return fail(PT_ERR_STATE, "viscosity not set (pt_op_set_eta_*)");
+  return PT_OK;
+}
+
+pt_status upload_diag_tables()
+{
+  static bool done[64] = {false};
+  int dev = 0;
+  PT_CUDA(cudaGetDevice(&dev));
+  if (dev < 64 && done[dev]) return PT_OK;
+  // dN_n/dxi_d at Gauss point q (tensor-product Q2 basis).
+  double b[3][3], db[3][3];
+  const double x[3] = {-q2::GS, 0.0, q2::GS};
+  for (int q = 0; q < 3; q++) {
+    const double t = x[q];
+    b[q][0] = 0.5 * t * (t - 1.0); b[q][1] = (1.0 + t) * (1.0 - t); b[q][2] = 0.5 * (1.0 + t) * t;
+    db[q][0] = t - 0.5; db[q][1] = -2.0 * t; db[q][2] = t + 0.5;
+  }
+  static double tab[27][27][3];
+  for (int a = 0; a < 3; a++)
+    for (int bq = 0; bq < 3; bq++)
+      for (int c = 0; c < 3; c++)
+        for (int k = 0; k < 3; k++)
+          for (int j = 0; j < 3; j++)
+            for (int i = 0; i < 3; i++) {
+              const int q = 9 * a + 3 * bq + c, n = 9 * k + 3 * j + i;
+              tab[q][n][0] = db[c][i] * b[bq][j] * b[a][k];
+              tab[q][n][1] = b[c][i] * db[bq][j] * b[a][k];
+              tab[q][n][2] = b[c][i] * b[bq][j] * db[a][k];
+            }
+  PT_CUDA(cudaMemcpyToSymbol(ptk::c_dN, tab, sizeof tab));
+  if (dev < 64) done[dev] = true;
+  return PT_OK;
+}
+
+// ---- A11 dispatch -----------------------------------------------------------
+
+template <typename T>
+pt_status launch_a11(pt_op *op, const T *coords, const T *eta, const T *u, T *y, bool masked)
+{
+  PT_CUDA(cudaMemsetAsync(y, 0, sizeof(T) * op->nvel, op->stream));
+  for (int c = 0; c < 8; c++) {
+    ptk::ColourGrid g = ptk::colour_grid(op->mx, op->my, op->mz, c);
+    const int64_t n = (int64_t)g.ncx * g.ncy * g.ncz;
+    if (n == 0) continue;
+    if (masked)
+      ptk::a11_colour_kernel<T, true><<<nblocks(n), TPB, 0, op->stream>>>(g, coords, eta, u, op->d_mask, y);
+    else
+      ptk::a11_colour_kernel<T, false><<<nblocks(n), TPB, 0, op->stream>>>(g, coords, eta, u, nullptr, y);
+    PT_LAUNCHED(op);
+  }
+  return PT_OK;
+}
+
+pt_status diag_d(pt_op *op, double *d)
+{
+  pt_status s = upload_diag_tables();
+  if (s != PT_OK) return s;
+  PT_CUDA(cudaMemsetAsync(d, 0, sizeof(double) * op->nvel, op->stream));
+  for (int c = 0; c < 8; c++) {
+    ptk::ColourGrid g = ptk::colour_grid(op->mx, op->my, op->mz, c);
+    const int64_t n = (int64_t)g.ncx * g.ncy * g.ncz;
+    if (n == 0) continue;
+    ptk::diag_colour_kernel<<<nblocks(n), TPB, 0, op->stream>>>(g, op->d_coords, op->d_eta, d);
+    PT_LAUNCHED(op);
+  }
+  return PT_OK;
+}
+
+pt_status a21_d(pt_op *op, const double *u, double *yp, bool masked)
+{
+  if (masked)
+    ptk::a21_kernel<true><<<nblocks(op->nel), TPB, 0, op->stream>>>(op->mx, op->my, op->mz, op->d_coords, u, op->d_mask, yp);
+  else
+    ptk::a21_kernel<false><<<nblocks(op->nel), TPB, 0, op->stream>>>(op->mx, op->my, op->mz, op->d_coords, u, nullptr, yp);
+  PT_LAUNCHED(op);
+  return PT_OK;
+}
+
+pt_status a12_d(pt_op *op, const double *p, double *yu)
+{
+  PT_CUDA(cudaMemsetAsync(yu, 0, sizeof(double) * op->nvel, op->stream));
+  for (int c = 0; c < 8; c++) {
+    ptk::ColourGrid g = ptk::colour_grid(op->mx, op->my, op->mz, c);
+    const int64_t n = (int64_t)g.ncx * g.ncy * g.ncz;
+    if (n == 0) continue;
+    ptk::a12_colour_kernel<<<nblocks(n), TPB, 0, op->stream>>>(g, op->d_coords, p, yu);
+    PT_LAUNCHED(op);
+  }
+  return PT_OK;
+}
+
+pt_status bc_copy(pt_op *op, const double *x, double *y)
+{
+  if (!op->has_mask) return PT_OK;
+  bc_copy_kernel<double><<<grid_stride_blocks(op->nvel), 256, 0, op->stream>>>(op->d_mask, x, y, op->nvel);
+  PT_LAUNCHED(op);
+  return PT_OK;
+}
+
+pt_status bc_copy32(pt_op *op, const float *x, float *y)
+{
+  if (!op->has_mask) return PT_OK;
+  bc_copy_kernel<float><<<grid_stride_blocks(op->nvel), 256, 0, op->stream>>>(op->d_mask, x, y, op->nvel);
+  PT_LAUNCHED(op);
+  return PT_OK;
+}
+
+pt_status bc_value(pt_op *op, double v, double *y)
+{
+  if (!op->has_mask) return PT_OK;
+  bc_value_kernel<<<grid_stride_blocks(op->nvel), 256, 0, op->stream>>>(op->d_mask, v, y, op->nvel);
+  PT_LAUNCHED(op);
+  return PT_OK;
+}
+
+// Host-pointer wrapper: copy nin doubles in, run f, copy nout doubles out, sync.
+template <typename F>
+pt_status host_call(pt_op *op, const double *in, int64_t nin, double *din, double *out, int64_t nout, double *dout, F f)
+{
+  if (!out) return fail(PT_ERR_BAD_ARG, "output pointer is NULL");
+  if (nin > 0) {
+    if (!in) return fail(PT_ERR_BAD_ARG, "input pointer is NULL");
+    PT_CUDA(cudaMemcpyAsync(din, in, sizeof(double) * nin, cudaMemcpyHostToDevice, op->stream));
+  }
+  pt_status s = f();
+  if (s != PT_OK) return s;
+  PT_CUDA(cudaMemcpyAsync(out, dout, sizeof(double) * nout, cudaMemcpyDeviceToHost, op->stream));
+  PT_CUDA(cudaStreamSynchronize(op->stream));
+  return PT_OK;
+}
+
+}  // namespace
+
+// ============================================================================
+extern "C" {
+
+const char *pt_last_error(void) { return g_err.c_str(); }
+const char *pt_version(void) { return "pt_b200 0.1 (sm_100a)"; }
+
+pt_status pt_op_create(const pt_mesh_desc *desc, pt_op **out)
+{
+  if (!desc || !out) return fail(PT_ERR_BAD_ARG, "NULL argument");
+  *out = nullptr;
+  if (desc->mx < 1 || desc->my < 1 || desc->mz < 1)
+    return fail(PT_ERR_BAD_ARG, "element counts must be >= 1 (got %d x %d x %d)", desc->mx, desc->my, desc->mz);
+  const int64_t nx = 2 * (int64_t)desc->mx + 1, ny = 2 * (int64_t)desc->my + 1, nz = 2 * (int64_t)desc->mz + 1;
+  const int64_t nnodes = nx * ny * nz;
+  if (nnodes > ((int64_t)1 << 40)) return fail(PT_ERR_BAD_ARG, "mesh too large");
+  pt_op *op = (pt_op *)calloc(1, sizeof(pt_op));
+  if (!op) return fail(PT_ERR_OOM, "host allocation failed");
+  op->mx = desc->mx; op->my = desc->my; op->mz = desc->mz;
+  op->nnodes = nnodes;
+  op->nvel = 3 * nnodes;
+  op->nel = (int64_t)desc->mx * desc->my * desc->mz;
+  op->npres = 4 * op->nel;
+  op->a11_kernel = A11_COLOUR;
+  cudaError_t e = cudaGetDevice(&op->device);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&op->stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) op->own_stream = true;
+  if (e == cudaSuccess) e = cudaMalloc(&op->d_coords, sizeof(double) * op->nvel);
+  if (e == cudaSuccess) e = cudaMalloc(&op->d_eta, sizeof(double) * 27 * op->nel);
+  if (e == cudaSuccess) e = cudaMalloc(&op->d_coords32, sizeof(float) * op->nvel);
+  if (e == cudaSuccess) e = cudaMalloc(&op->d_eta32, sizeof(float) * 27 * op->nel);
+  if (e == cudaSuccess) e = cudaMalloc(&op->d_mask, op->nvel);
+  if (e == cudaSuccess) e = cudaMemset(op->d_mask, 0, op->nvel);
+  if (e != cudaSuccess) {
+    pt_status s = fail(e == cudaErrorMemoryAllocation ? PT_ERR_OOM : PT_ERR_CUDA, "pt_op_create: %s",
+                       cudaGetErrorString(e));
+    pt_op_destroy(op);
+    return s;
+  }
+  *out = op;
+  return PT_OK;
+}
+
+pt_status pt_op_destroy(pt_op *op)
+{
+  if (!op) return PT_OK;
+  if (op->stream) cudaStreamSynchronize(op->stream);
+  cudaFree(op->d_coords); cudaFree(op->d_eta);
+  cudaFree(op->d_coords32); cudaFree(op->d_eta32);
+  cudaFree(op->d_mask);
+  cudaFree(op->d_u); cudaFree(op->d_y); cudaFree(op->d_p);
+  if (op->own_stream && op->stream) cudaStreamDestroy(op->stream);
+  free(op);
+  return PT_OK;
+}
+
+pt_status pt_op_set_stream(pt_op *op, void *stream)
+{
+  if (!op) return fail(PT_ERR_BAD_ARG, "op is NULL");
+  PT_CUDA(cudaStreamSynchronize(op->stream));
+  if (op->own_stream) PT_CUDA(cudaStreamDestroy(op->stream));
+  op->own_stream = false;
+  op->stream = (cudaStream_t)stream;
+  if (!stream) {
+    PT_CUDA(cudaStreamCreateWithFlags(&op->stream, cudaStreamNonBlocking));
+    op->own_stream = true;
+  }
+  return PT_OK;
+}
+
+pt_status pt_op_get_sizes(const pt_op *op, int64_t *nvel, int64_t *npres, int64_t *nel)
+{
+  if (!op) return fail(PT_ERR_BAD_ARG, "op is NULL");
+  if (nvel) *nvel = op->nvel;
+  if (npres) *npres = op->npres;
+  if (nel) *nel = op->nel;
+  return PT_OK;
+}
+
+static pt_status finish_coords(pt_op *op)
+{
+  to_f32_kernel<<<grid_stride_blocks(op->nvel), 256, 0, op->stream>>>(op->d_coords, op->d_coords32, op->nvel);
+  PT_LAUNCHED(op);
+  op->has_coords = true;
+  return PT_OK;
+}
+
+static pt_status finish_eta(pt_op *op)
+{
+  to_f32_kernel<<<grid_stride_blocks(27 * op->nel), 256, 0, op->stream>>>(op->d_eta, op->d_eta32, 27 * op->nel);
+  PT_LAUNCHED(op);
+  op->has_eta = true;
+  return PT_OK;
+}
+
+pt_status pt_op_set_coords_h(pt_op *op, const double *coords)
+{
+  if (!op || !coords) return fail(PT_ERR_BAD_ARG, "NULL argument");
+  PT_CUDA(cudaMemcpyAsync(op->d_coords, coords, sizeof(double) * op->nvel, cudaMemcpyHostToDevice, op->stream));
+  pt_status s = finish_coords(op);
+  if (s != PT_OK) return s;
+  PT_CUDA(cudaStreamSynchronize(op->stream));
+  return PT_OK;
+}
+
+pt_status pt_op_set_coords_d(pt_op *op, const double *coords)
+{
+  if (!op || !coords) return fail(PT_ERR_BAD_ARG, "NULL argument");
+  PT_CUDA(cudaMemcpyAsync(op->d_coords, coords, sizeof(double) * op->nvel, cudaMemcpyDeviceToDevice, op->stream));
+  return finish_coords(op);
+}
+
+pt_status pt_op_set_eta_h(pt_op *op, const double *eta)
+{
+  if (!op || !eta) return fail(PT_ERR_BAD_ARG, "NULL argument");
+  PT_CUDA(cudaMemcpyAsync(op->d_eta, eta, sizeof(double) * 27 * op->nel, cudaMemcpyHostToDevice, op->stream));
+  pt_status s = finish_eta(op);
+  if (s != PT_OK) return s;
+  PT_CUDA(cudaStreamSynchronize(op->stream));
+  return PT_OK;
+}
+
+pt_status pt_op_set_eta_d(pt_op *op, const double *eta)
+{
+  if (!op || !eta) return fail(PT_ERR_BAD_ARG, "NULL argument");
+  PT_CUDA(cudaMemcpyAsync(op->d_eta, eta, sizeof(double) * 27 * op->nel, cudaMemcpyDeviceToDevice, op->stream));
+  return finish_eta(op);
+}
+
+pt_status pt_op_set_bc_mask_h(pt_op *op, const uint8_t *mask)
+{
+  if (!op) return fail(PT_ERR_BAD_ARG, "op is NULL");
+  if (!mask) {
+    PT_CUDA(cudaMemsetAsync(op->d_mask, 0, op->nvel, op->stream));
+    op->has_mask = false;
+  } else {
+    PT_CUDA(cudaMemcpyAsync(op->d_mask, mask, op->nvel, cudaMemcpyHostToDevice, op->stream));
+    op->has_mask = true;
+  }
+  PT_CUDA(cudaStreamSynchronize(op->stream));
+  return PT_OK;
+}
+
+static pt_status ensure_staging(pt_op *op)
+{
+  if (!op->d_u) PT_CUDA(cudaMalloc(&op->d_u, sizeof(double) * op->nvel));
+  if (!op->d_y) PT_CUDA(cudaMalloc(&op->d_y, sizeof(double) * op->nvel));
+  if (!op->d_p) PT_CUDA(cudaMalloc(&op->d_p, sizeof(double) * op->npres));
+  return PT_OK;
+}
+
+// ---- SpMVOp level -----------------------------------------------------------
+
+pt_status pt_a11_apply_d(pt_op *op, const double *u, double *y)
+{
+  pt_status s = check_ready(op, true);
+  if (s != PT_OK) return s;
+  if (!u || !y) return fail(PT_ERR_BAD_ARG, "NULL vector");
+  return launch_a11<double>(op, op->d_coords, op->d_eta, u, y, false);
+}
+
+pt_status pt_a11_apply_h(pt_op *op, const double *u, double *y)
+{
+  pt_status s = check_ready(op, true);
+  if (s != PT_OK) return s;
+  if ((s = ensure_staging(op)) != PT_OK) return s;
+  return host_call(op, u, op->nvel, op->d_u, y, op->nvel, op->d_y,
+                   [&]() { return launch_a11<double>(op, op->d_coords, op->d_eta, op->d_u, op->d_y, false); });
+}
+
+pt_status pt_a11_apply_f32_d(pt_op *op, const float *u, float *y)
+{
+  pt_status s = check_ready(op, true);
+  if (s != PT_OK) return s;
+  if (!u || !y) return fail(PT_ERR_BAD_ARG, "NULL vector");
+  return launch_a11<float>(op, op->d_coords32, op->d_eta32, u, y, false);
+}
+
+pt_status pt_a11_diag_d(pt_op *op, double *d)
+{
+  pt_status s = check_ready(op, true);
+  if (s != PT_OK) return s;
+  if (!d) return fail(PT_ERR_BAD_ARG, "NULL vector");
+  return diag_d(op, d);
+}
+
+pt_status pt_a11_diag_h(pt_op *op, double *d)
+{
+  pt_status s = check_ready(op, true);
+  if (s != PT_OK) return s;
+  if ((s = ensure_staging(op)) != PT_OK) return s;
+  return host_call(op, nullptr, 0, nullptr, d, op->nvel, op->d_y, [&]() { return diag_d(op, op->d_y); });
+}
+
+pt_status pt_a21_apply_d(pt_op *op, const double *u, double *yp)
+{
+  pt_status s = check_ready(op, false);
+  if (s != PT_OK) return s;
+  if (!u || !yp) return fail(PT_ERR_BAD_ARG, "NULL vector");
+  return a21_d(op, u, yp, false);
+}
+
+pt_status pt_a21_apply_h(pt_op *op, const double *u, double *yp)
+{
+  pt_status s = check_ready(op, false);
+  if (s != PT_OK) return s;
+  if ((s = ensure_staging(op)) != PT_OK) return s;
+  return host_call(op, u, op->nvel, op->d_u, yp, op->npres, op->d_p, [&]() { return a21_d(op, op->d_u, op->d_p, false); });
+}
+
+pt_status pt_a12_apply_d(pt_op *op, const double *p, double *yu)
+{
+  pt_status s = check_ready(op, false);
+  if (s != PT_OK) return s;
+  if (!p || !yu) return fail(PT_ERR_BAD_ARG, "NULL vector");
+  return a12_d(op, p, yu);
+}
+
+pt_status pt_a12_apply_h(pt_op *op, const double *p, double *yu)
+{
+  pt_status s = check_ready(op, false);
+  if (s != PT_OK) return s;
+  if ((s = ensure_staging(op)) != PT_OK) return s;
+  return host_call(op, p, op->npres, op->d_p, yu, op->nvel, op->d_y, [&]() { return a12_d(op, op->d_p, op->d_y); });
+}
+
+// ---- MatShell level -----------------------------------------------------------
+
+pt_status pt_matmult_a11_d(pt_op *op, const double *x, double *y)
+{
+  pt_status s = check_ready(op, true);
+  if (s != PT_OK) return s;
+  if (!x || !y) return fail(PT_ERR_BAD_ARG, "NULL vector");
+  if (x == y) return fail(PT_ERR_BAD_ARG, "x and y must not alias");
+  if ((s = launch_a11<double>(op, op->d_coords, op->d_eta, x, y, op->has_mask)) != PT_OK) return s;
+  return bc_copy(op, x, y);
+}
+
+pt_status pt_matmult_a11_h(pt_op *op, const double *x, double *y)
+{
+  pt_status s = check_ready(op, true);
+  if (s != PT_OK) return s;
+  if ((s = ensure_staging(op)) != PT_OK) return s;
+  return host_call(op, x, op->nvel, op->d_u, y, op->nvel, op->d_y,
+                   [&]() { return pt_matmult_a11_d(op, op->d_u, op->d_y); });
+}
+
+pt_status pt_matmult_a11_f32_d(pt_op *op, const float *x, float *y)
+{
+  pt_status s = check_ready(op, true);
+  if (s != PT_OK) return s;
+  if (!x || !y) return fail(PT_ERR_BAD_ARG, "NULL vector");
+  if (x == y) return fail(PT_ERR_BAD_ARG, "x and y must not alias");
+  if ((s = launch_a11<float>(op, op->d_coords32, op->d_eta32, x, y, op->has_mask)) != PT_OK) return s;
+  return bc_copy32(op, x, y);
+}
+
+pt_status pt_getdiag_a11_d(pt_op *op, double *d)
+{
+  pt_status s = pt_a11_diag_d(op, d);
+  if (s != PT_OK) return s;
+  return bc_value(op, 1.0, d);
+}
+
+pt_status pt_getdiag_a11_h(pt_op *op, double *d)
+{
+  pt_status s = check_ready(op, true);
+  if (s != PT_OK) return s;
+  if ((s = ensure_staging(op)) != PT_OK) return s;
+  return host_call(op, nullptr, 0, nullptr, d, op->nvel, op->d_y, [&]() { return pt_getdiag_a11_d(op, op->d_y); });
+}
+
+pt_status pt_matmult_a12_d(pt_op *op, const double *p, double *yu)
+{
+  pt_status s = pt_a12_apply_d(op, p, yu);
+  if (s != PT_OK) return s;
+  return bc_value(op, 0.0, yu);
+}
+
+pt_status pt_matmult_a12_h(pt_op *op, const double *p, double *yu)
+{
+  pt_status s = check_ready(op, false);
+  if (s != PT_OK) return s;
+  if ((s = ensure_staging(op)) != PT_OK) return s;
+  return host_call(op, p, op->npres, op->d_p, yu, op->nvel, op->d_y, [&]() { return pt_matmult_a12_d(op, op->d_p, op->d_y); });
+}
+
+pt_status pt_matmult_a21_d(pt_op *op, const double *u, double *yp)
+{
+  pt_status s = check_ready(op, false);
+  if (s != PT_OK) return s;
+  if (!u || !yp) return fail(PT_ERR_BAD_ARG, "NULL vector");
+  return a21_d(op, u, yp, op->has_mask);
+}
+
+pt_status pt_matmult_a21_h(pt_op *op, const double *u, double *yp)
+{
+  pt_status s = check_ready(op, false);
+  if (s != PT_OK) return s;
+  if ((s = ensure_staging(op)) != PT_OK) return s;
+  return host_call(op, u, op->nvel, op->d_u, yp, op->npres, op->d_p, [&]() { return pt_matmult_a21_d(op, op->d_u, op->d_p); });
+}
+
+pt_status pt_op_set_a11_kernel(pt_op *op, const char *name)
+{
+  if (!op || !name) return fail(PT_ERR_BAD_ARG, "NULL argument");
+  if (!strcmp(name, "b200")) op->a11_kernel = A11_COLOUR;
+  else if (!strcmp(name, "b200_colour")) op->a11_kernel = A11_COLOUR;
+  else return fail(PT_ERR_BAD_ARG, "No -a11_op %s", name);
+  return PT_OK;
+}
+
+const char *pt_op_get_a11_kernel(const pt_op *op)
+{
+  if (!op) return "";
+  return op->a11_kernel == A11_STREAM ? "b200" : "b200_colour";
+}
+
+int64_t pt_op_launch_count(const pt_op *op) { return op ? op->launches : 0; }
+void pt_op_reset_launch_count(pt_op *op)
+{
+  if (op) op->launches = 0;
+}
+
+}  // extern "C"

@@ -1,0 +1,108 @@
+"""ctypes binding of libpt_b200.so (the C ABI in include/pt_b200.h).
+
+Loading fails loudly: there is no CPU fallback anywhere in this package.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+from . import build as _build
+
+PT_OK = 0
+STATUS = {0: "PT_OK", 1: "PT_ERR_BAD_ARG", 2: "PT_ERR_OOM", 3: "PT_ERR_CUDA",
+          4: "PT_ERR_TIMEOUT", 5: "PT_ERR_STATE", 6: "PT_ERR_UNSUPPORTED"}
+
+
+class PtError(RuntimeError):
+    def __init__(self, status: int, where: str, msg: str):
+        super().__init__(f"{where}: {STATUS.get(status, status)}: {msg}")
+        self.status = status
+
+
+class MeshDesc(ctypes.Structure):
+    _fields_ = [("mx", ctypes.c_int32), ("my", ctypes.c_int32), ("mz", ctypes.c_int32)]
+
+
+_vp = ctypes.c_void_p
+_i64p = ctypes.POINTER(ctypes.c_int64)
+
+# name -> argtypes (all return int status unless listed in _RESTYPES)
+SIGNATURES = {
+    "pt_op_create": [ctypes.POINTER(MeshDesc), ctypes.POINTER(_vp)],
+    "pt_op_destroy": [_vp],
+    "pt_op_set_stream": [_vp, _vp],
+    "pt_op_get_sizes": [_vp, _i64p, _i64p, _i64p],
+    "pt_op_set_coords_h": [_vp, _vp],
+    "pt_op_set_coords_d": [_vp, _vp],
+    "pt_op_set_eta_h": [_vp, _vp],
+    "pt_op_set_eta_d": [_vp, _vp],
+    "pt_op_set_bc_mask_h": [_vp, _vp],
+    "pt_a11_apply_h": [_vp, _vp, _vp],
+    "pt_a11_apply_d": [_vp, _vp, _vp],
+    "pt_a11_apply_f32_d": [_vp, _vp, _vp],
+    "pt_a11_diag_h": [_vp, _vp],
+    "pt_a11_diag_d": [_vp, _vp],
+    "pt_a21_apply_h": [_vp, _vp, _vp],
+    "pt_a21_apply_d": [_vp, _vp, _vp],
+    "pt_a12_apply_h": [_vp, _vp, _vp],
+    "pt_a12_apply_d": [_vp, _vp, _vp],
+    "pt_matmult_a11_h": [_vp, _vp, _vp],
+    "pt_matmult_a11_d": [_vp, _vp, _vp],
+    "pt_matmult_a11_f32_d": [_vp, _vp, _vp],
+    "pt_getdiag_a11_h": [_vp, _vp],
+    "pt_getdiag_a11_d": [_vp, _vp],
+    "pt_matmult_a12_h": [_vp, _vp, _vp],
+    "pt_matmult_a12_d": [_vp, _vp, _vp],
+    "pt_matmult_a21_h": [_vp, _vp, _vp],
+    "pt_matmult_a21_d": [_vp, _vp, _vp],
+    "pt_op_set_a11_kernel": [_vp, ctypes.c_char_p],
+    "pt_op_get_a11_kernel": [_vp],
+    "pt_op_launch_count": [_vp],
+    "pt_op_reset_launch_count": [_vp],
+    "pt_last_error": [],
+    "pt_version": [],
+}
+_RESTYPES = {
+    "pt_last_error": ctypes.c_char_p,
+    "pt_version": ctypes.c_char_p,
+    "pt_op_get_a11_kernel": ctypes.c_char_p,
+    "pt_op_launch_count": ctypes.c_int64,
+    "pt_op_reset_launch_count": None,
+}
+
+_lib = None
+
+
+def lib_path() -> str:
+    return _build.LIB
+
+
+def load(build_if_missing: bool = True):
+    """Load libpt_b200.so, building it in-tree first when absent or stale."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    path = _build.LIB
+    if build_if_missing and _build.needs_build():
+        _build.build()
+    if not os.path.exists(path):
+        raise ImportError(f"libpt_b200.so not built ({path}); run `python -m pt_b200.build`")
+    lib = ctypes.CDLL(path)
+    for name, args in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.argtypes = args
+        fn.restype = _RESTYPES.get(name, ctypes.c_int)
+    _lib = lib
+    return lib
+
+
+def check(status: int, where: str):
+    if status != PT_OK:
+        raise PtError(status, where, load().pt_last_error().decode(errors="replace"))
+
+
+def call(name: str, *args):
+    st = getattr(load(), name)(*args)
+    check(st, name)
+    return st

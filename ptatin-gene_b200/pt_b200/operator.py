@@ -1,0 +1,210 @@
+"""Host-side mirror of pTatin3D's matrix-free Stokes operator interface.
+
+``MatStokesMF`` plays the role of the reference's ``MatA11MF`` / ``MatStokesMF``
+contexts (include/stokes_operators.h:34-64) for one rank: it is created with
+an ``a11_op`` name (the ``-a11_op`` switch of src/stokes_operators.c:123-154),
+set up with the mesh data, and exposes
+
+* the SpMVOp-level element loops under the reference's names
+  (``MFStokesWrapper_A11``, ``MFStokesWrapper_diagA11``, ``MFStokesWrapper_A12``,
+  ``MFStokesWrapper_A21``): caller-zeroed Dirichlet input, unassembled output;
+* the MatShell-level operators (``MatMult_MFStokes_A11``,
+  ``MatGetDiagonal_MFStokes_A11``, ``MatMult_MFStokes_A12``,
+  ``MatMult_MFStokes_A21``) with the reference's BC semantics.
+
+Vectors may be numpy arrays (host path: the library copies in and out) or
+CUDA ``torch`` tensors (device path, asynchronous on the op's stream unless
+``sync=True``).  Every call goes through libpt_b200.so; there is no CPU path.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _capi
+
+try:  # torch is plumbing only (device memory, streams); optional on CPU hosts
+    import torch
+except Exception:  # pragma: no cover
+    torch = None
+
+A11_OPS = ("b200", "b200_colour")
+
+
+def _is_dev(a) -> bool:
+    return torch is not None and isinstance(a, torch.Tensor) and a.is_cuda
+
+
+def _hptr(a: np.ndarray, dtype):
+    if not isinstance(a, np.ndarray) or a.dtype != dtype or not a.flags["C_CONTIGUOUS"]:
+        raise TypeError(f"expected a C-contiguous numpy {np.dtype(dtype).name} array")
+    return ctypes.c_void_p(a.ctypes.data)
+
+
+def _dptr(t, dtype):
+    if t.dtype != dtype or not t.is_contiguous():
+        raise TypeError(f"expected a contiguous CUDA tensor of {dtype}")
+    return ctypes.c_void_p(t.data_ptr())
+
+
+class MatStokesMF:
+    """One rank's Q2-P1disc Stokes operator on a structured box of mx*my*mz elements."""
+
+    def __init__(self, mx: int, my: int, mz: int, a11_op: str = "b200", stream=None):
+        self._lib = _capi.load()
+        self.dims = (int(mx), int(my), int(mz))
+        h = ctypes.c_void_p()
+        _capi.call("pt_op_create", ctypes.byref(_capi.MeshDesc(*self.dims)), ctypes.byref(h))
+        self._h = h
+        nv, npr, nel = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64()
+        _capi.call("pt_op_get_sizes", h, ctypes.byref(nv), ctypes.byref(npr), ctypes.byref(nel))
+        self.nvel, self.npres, self.nel = nv.value, npr.value, nel.value
+        self.set_a11_op(a11_op)
+        if stream is not None:
+            self.set_stream(stream)
+
+    # -- lifecycle ---------------------------------------------------------
+    def Destroy(self):
+        if getattr(self, "_h", None):
+            _capi.call("pt_op_destroy", self._h)
+            self._h = None
+
+    def __del__(self):  # pragma: no cover
+        try:
+            self.Destroy()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.Destroy()
+
+    @property
+    def handle(self):
+        return self._h
+
+    def set_stream(self, stream):
+        """Use a torch.cuda.Stream (or a raw cudaStream_t int) for all work."""
+        raw = stream.cuda_stream if hasattr(stream, "cuda_stream") else int(stream)
+        _capi.call("pt_op_set_stream", self._h, ctypes.c_void_p(raw))
+
+    def set_a11_op(self, name: str):
+        _capi.call("pt_op_set_a11_kernel", self._h, name.encode())
+
+    @property
+    def a11_op(self) -> str:
+        return self._lib.pt_op_get_a11_kernel(self._h).decode()
+
+    def launch_count(self) -> int:
+        return int(self._lib.pt_op_launch_count(self._h))
+
+    def reset_launch_count(self):
+        self._lib.pt_op_reset_launch_count(self._h)
+
+    # -- setup (MatA11MFSetup / SpMVOp_SetUp) -----------------------------
+    def SetUp(self, coords, eta=None, mask=None):
+        self.set_coords(coords)
+        if eta is not None:
+            self.set_eta(eta)
+        self.set_bc_mask(mask)
+        return self
+
+    def set_coords(self, coords):
+        if _is_dev(coords):
+            _capi.call("pt_op_set_coords_d", self._h, _dptr(coords, torch.float64))
+        else:
+            c = np.ascontiguousarray(coords, dtype=np.float64)
+            if c.size != self.nvel:
+                raise ValueError(f"coords has {c.size} entries, expected {self.nvel}")
+            _capi.call("pt_op_set_coords_h", self._h, _hptr(c, np.float64))
+
+    def set_eta(self, eta):
+        if _is_dev(eta):
+            _capi.call("pt_op_set_eta_d", self._h, _dptr(eta, torch.float64))
+        else:
+            e = np.ascontiguousarray(eta, dtype=np.float64)
+            if e.size != 27 * self.nel:
+                raise ValueError(f"eta has {e.size} entries, expected {27 * self.nel}")
+            _capi.call("pt_op_set_eta_h", self._h, _hptr(e, np.float64))
+
+    def set_bc_mask(self, mask):
+        if mask is None:
+            _capi.call("pt_op_set_bc_mask_h", self._h, ctypes.c_void_p(None))
+            return
+        m = np.ascontiguousarray(mask, dtype=np.uint8)
+        if m.size != self.nvel:
+            raise ValueError(f"mask has {m.size} entries, expected {self.nvel}")
+        _capi.call("pt_op_set_bc_mask_h", self._h, _hptr(m, np.uint8))
+
+    # -- generic dispatch ----------------------------------------------------
+    def _apply(self, base: str, x, nout: int, out=None, dtype=np.float64):
+        if _is_dev(x):
+            tdt = torch.float64 if dtype == np.float64 else torch.float32
+            if out is None:
+                out = torch.empty(nout, dtype=tdt, device=x.device)
+            _capi.call(base + "_d", self._h, _dptr(x, tdt), _dptr(out, tdt))
+            return out
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        if out is None:
+            out = np.empty(nout, dtype=np.float64)
+        _capi.call(base + "_h", self._h, _hptr(x, np.float64), _hptr(out, np.float64))
+        return out
+
+    def _check_len(self, x, n, what):
+        if (x.numel() if _is_dev(x) else np.size(x)) != n:
+            raise ValueError(f"{what} has the wrong length (expected {n})")
+
+    # -- SpMVOp level --------------------------------------------------------
+    def MFStokesWrapper_A11(self, ufield, Yu=None):
+        self._check_len(ufield, self.nvel, "ufield")
+        if _is_dev(ufield) and ufield.dtype == torch.float32:
+            if Yu is None:
+                Yu = torch.empty_like(ufield)
+            _capi.call("pt_a11_apply_f32_d", self._h, _dptr(ufield, torch.float32), _dptr(Yu, torch.float32))
+            return Yu
+        return self._apply("pt_a11_apply", ufield, self.nvel, Yu)
+
+    def MFStokesWrapper_diagA11(self, Yu=None):
+        if Yu is not None and _is_dev(Yu):
+            _capi.call("pt_a11_diag_d", self._h, _dptr(Yu, torch.float64))
+            return Yu
+        out = np.empty(self.nvel) if Yu is None else Yu
+        _capi.call("pt_a11_diag_h", self._h, _hptr(out, np.float64))
+        return out
+
+    def MFStokesWrapper_A12(self, Xp, Yu=None):
+        self._check_len(Xp, self.npres, "Xp")
+        return self._apply("pt_a12_apply", Xp, self.nvel, Yu)
+
+    def MFStokesWrapper_A21(self, Xu, Yp=None):
+        self._check_len(Xu, self.nvel, "Xu")
+        return self._apply("pt_a21_apply", Xu, self.npres, Yp)
+
+    # -- MatShell level ------------------------------------------------------
+    def MatMult_MFStokes_A11(self, X, Y=None):
+        self._check_len(X, self.nvel, "X")
+        if _is_dev(X) and X.dtype == torch.float32:
+            if Y is None:
+                Y = torch.empty_like(X)
+            _capi.call("pt_matmult_a11_f32_d", self._h, _dptr(X, torch.float32), _dptr(Y, torch.float32))
+            return Y
+        return self._apply("pt_matmult_a11", X, self.nvel, Y)
+
+    def MatGetDiagonal_MFStokes_A11(self, X=None):
+        if X is not None and _is_dev(X):
+            _capi.call("pt_getdiag_a11_d", self._h, _dptr(X, torch.float64))
+            return X
+        out = np.empty(self.nvel) if X is None else X
+        _capi.call("pt_getdiag_a11_h", self._h, _hptr(out, np.float64))
+        return out
+
+    def MatMult_MFStokes_A12(self, X, Y=None):
+        self._check_len(X, self.npres, "X")
+        return self._apply("pt_matmult_a12", X, self.nvel, Y)
+
+    def MatMult_MFStokes_A21(self, X, Y=None):
+        self._check_len(X, self.nvel, "X")
+        return self._apply("pt_matmult_a21", X, self.npres, Y)

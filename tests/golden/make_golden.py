@@ -1,0 +1,66 @@
+"""Generates the golden fixtures in this directory from the reference's own code.
+
+The outputs come from oracle/_ref/libptref.so, i.e. the reference's
+src/stokes_operators_{tensor,avx,mf}.c and src/element_utils_q{1,2}.c compiled
+unmodified (oracle/Makefile, Route A).  Inputs are seeded synthetic box meshes
+(ptatin-gene_b200/pt_b200/mesh.py).  Re-run after changing either:
+
+    python tests/golden/make_golden.py
+
+Each fixture stores the inputs and the reference outputs of
+  A11 via "tensor", "avx" and "ref" (MFStokesWrapper_A11_*),
+  diag(A11) (MFStokesWrapper_diagA11),
+  A21 = B u (MFStokesWrapper_A21),
+  A12 = B^T p via "avx" and "ref" (MFStokesWrapper_A12_AVX / MFStokesWrapper_A12),
+all as unassembled local sums on one rank (local == global numbering).
+"""
+from __future__ import annotations
+
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, REPO)
+sys.path.insert(0, os.path.join(REPO, "ptatin-gene_b200"))
+
+import oracle  # noqa: E402
+from pt_b200 import mesh as M  # noqa: E402
+
+CASES = {
+    # name: (workload, u seed, p seed, use the reference's X+Y+Z+c+3 vector)
+    "c0_8x8x8": ("c0", 11, 12, False),
+    "box_3x2x4": ("box:3,2,4", 21, 22, False),
+    "box_1x1x3": ("box:1,1,3", 31, 32, False),
+    "box_5x1x2_refvec": ("box:5,1,2", 41, 42, True),
+}
+
+
+def make(name, workload, useed, pseed, refvec):
+    m, eta, mask = M.problem(workload)
+    u = M.reference_test_vector(m) if refvec else M.uniform_vec(m.nvel, useed)
+    p = M.uniform_vec(m.npres, pseed)
+    uz = u.copy()
+    uz[mask.astype(bool)] = 0.0
+    r = oracle.RefCPU()
+    out = dict(
+        dims=np.array(m.dims, dtype=np.int32), coords=m.coords, eta=eta, mask=mask, u=u, p=p,
+        a11_tensor=r.a11(m.dims, m.coords, eta, uz, "tensor"),
+        a11_avx=r.a11(m.dims, m.coords, eta, uz, "avx"),
+        a11_ref=r.a11(m.dims, m.coords, eta, uz, "ref"),
+        diag=r.diag(m.dims, m.coords, eta),
+        a21=r.a21(m.dims, m.coords, uz),
+        a12_avx=r.a12(m.dims, m.coords, p, "avx"),
+        a12_ref=r.a12(m.dims, m.coords, p, "ref"),
+    )
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
+
+
+if __name__ == "__main__":
+    if not oracle.RefCPU.available():
+        oracle.build()
+    for name, args in CASES.items():
+        make(name, *args)
+        print("wrote", name)

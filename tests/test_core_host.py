@@ -1,0 +1,42 @@
+"""The kernels' per-element arithmetic (csrc/q2_core.cuh) compiled for the host
+with g++ and checked against the oracle -- the GPU kernels' algorithm is
+validated here without a GPU."""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from conftest import PKG_ROOT, REPO, relerr
+from pt_b200 import mesh as M
+
+
+@pytest.fixture(scope="module")
+def core(tmp_path_factory):
+    out = tmp_path_factory.mktemp("core") / "libcore.so"
+    src = os.path.join(REPO, "tests", "core_host_check.cpp")
+    subprocess.run(["g++", "-O2", "-fPIC", "-shared", "-I", os.path.join(PKG_ROOT, "csrc"), src, "-o", str(out)],
+                   check=True)
+    lib = ctypes.CDLL(str(out))
+    dp = ctypes.POINTER(ctypes.c_double)
+    for f in ("core_a11_f64", "core_a11_f32"):
+        getattr(lib, f).argtypes = [ctypes.c_int] * 3 + [dp] * 4
+    return lib
+
+
+def _p(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+@pytest.mark.parametrize("workload", ["c0", "box:1,1,1", "box:3,2,4", "box:5,1,2"])
+def test_core_a11_matches_oracle(core, ora, workload):
+    m, eta, _ = M.problem(workload)
+    u = M.uniform_vec(m.nvel, 3)
+    ref = ora.a11(m.dims, m.coords, eta, u)
+    y = np.zeros(m.nvel)
+    core.core_a11_f64(*m.dims, _p(m.coords), _p(eta), _p(u), _p(y))
+    assert relerr(y, ref) < 1e-13
+    y32 = np.zeros(m.nvel)
+    core.core_a11_f32(*m.dims, _p(m.coords), _p(eta), _p(u), _p(y32))
+    assert relerr(y32, ref) < 5e-5

@@ -1,0 +1,157 @@
+"""GPU parity: libpt_b200.so (through its C ABI) against the reference's own
+outputs (golden fixtures) and the oracle.
+
+Tolerances (relative, ||y - y_ref||_inf / ||y_ref||_inf):
+  FP64 operators  1e-12   (the project's parity bar)
+  FP32 A11        5e-5    (FP32 arithmetic and accumulation, eta contrast <= 1e4)
+"""
+import numpy as np
+import pytest
+
+from conftest import golden_names, load_golden, relerr
+from pt_b200 import mesh as M
+
+pytestmark = pytest.mark.gpu
+
+TOL64 = 1e-12
+TOL32 = 5e-5
+
+
+@pytest.fixture(scope="module")
+def torch_cuda():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.fail("CUDA device required for -m gpu tests")
+    return torch
+
+
+def make_op(m, eta=None, mask=None, a11_op="b200"):
+    from pt_b200 import MatStokesMF
+    op = MatStokesMF(*m.dims, a11_op=a11_op)
+    op.SetUp(m.coords, eta, mask)
+    return op
+
+
+@pytest.mark.parametrize("a11_op", ["b200", "b200_colour"])
+@pytest.mark.parametrize("name", golden_names())
+def test_spmvop_level_matches_reference(torch_cuda, name, a11_op):
+    g = load_golden(name)
+    m = M.BoxMesh(*(int(v) for v in g["dims"]), g["coords"])
+    uz = g["u"].copy()
+    uz[g["mask"].astype(bool)] = 0.0
+    with make_op(m, g["eta"], None, a11_op) as op:
+        assert relerr(op.MFStokesWrapper_A11(uz), g["a11_tensor"]) < TOL64
+        assert relerr(op.MFStokesWrapper_A11(uz), g["a11_avx"]) < TOL64
+        assert relerr(op.MFStokesWrapper_diagA11(), g["diag"]) < TOL64
+        assert relerr(op.MFStokesWrapper_A21(uz), g["a21"]) < TOL64
+        assert relerr(op.MFStokesWrapper_A12(g["p"]), g["a12_avx"]) < TOL64
+
+
+@pytest.mark.parametrize("workload", ["c0", "box:3,2,4", "box:1,1,1", "box:1,2,3", "box:7,5,3", "box:33,2,2",
+                                      "box:2,40,1", "box:64,3,1"])
+def test_matshell_level_matches_oracle(torch_cuda, ora, workload):
+    m, eta, mask = M.problem(workload, seed=5)
+    x = M.uniform_vec(m.nvel, 6)
+    p = M.uniform_vec(m.npres, 7)
+    with make_op(m, eta, mask) as op:
+        assert relerr(op.MatMult_MFStokes_A11(x), ora.matmult_a11(m.dims, m.coords, eta, mask, x)) < TOL64
+        assert relerr(op.MatGetDiagonal_MFStokes_A11(), ora.getdiag_a11(m.dims, m.coords, eta, mask)) < TOL64
+        assert relerr(op.MatMult_MFStokes_A12(p), ora.matmult_a12(m.dims, m.coords, mask, p)) < TOL64
+        assert relerr(op.MatMult_MFStokes_A21(x), ora.matmult_a21(m.dims, m.coords, mask, x)) < TOL64
+        # Dirichlet rows are exact copies (BCListInsertDirichlet_MatMult, scale 1)
+        y = op.MatMult_MFStokes_A11(x)
+        bc = mask.astype(bool)
+        assert np.array_equal(y[bc], x[bc])
+
+
+def test_device_and_host_paths_agree_bitwise(torch_cuda):
+    torch = torch_cuda
+    m, eta, mask = M.problem("box:9,6,5", seed=2)
+    x = M.uniform_vec(m.nvel, 3)
+    with make_op(m, eta, mask) as op:
+        yh = op.MatMult_MFStokes_A11(x)
+        xd = torch.from_numpy(x).cuda()
+        yd = op.MatMult_MFStokes_A11(xd)
+        torch.cuda.synchronize()
+        assert np.array_equal(yh, yd.cpu().numpy())
+
+
+def test_apply_is_deterministic(torch_cuda):
+    """No atomics: repeated applies are bitwise identical."""
+    torch = torch_cuda
+    m, eta, mask = M.problem("box:17,9,6", seed=4)
+    with make_op(m, eta, mask) as op:
+        xd = torch.from_numpy(M.uniform_vec(m.nvel, 5)).cuda()
+        y1 = op.MatMult_MFStokes_A11(xd).clone()
+        y2 = op.MatMult_MFStokes_A11(xd).clone()
+        torch.cuda.synchronize()
+        assert torch.equal(y1, y2)
+
+
+def test_kernels_agree(torch_cuda):
+    """The tuned and the 8-colour A11 kernels agree to FP64 rounding."""
+    torch = torch_cuda
+    m, eta, mask = M.problem("box:40,7,5", seed=8)
+    xd = torch.from_numpy(M.uniform_vec(m.nvel, 9)).cuda()
+    with make_op(m, eta, mask, "b200") as a, make_op(m, eta, mask, "b200_colour") as b:
+        ya = a.MatMult_MFStokes_A11(xd).cpu().numpy()
+        yb = b.MatMult_MFStokes_A11(xd).cpu().numpy()
+        assert relerr(ya, yb) < 1e-14
+
+
+@pytest.mark.parametrize("workload", ["c0", "box:7,5,3"])
+def test_fp32_apply(torch_cuda, ora, workload):
+    torch = torch_cuda
+    m, eta, mask = M.problem(workload, seed=1)
+    x = M.uniform_vec(m.nvel, 2)
+    ref = ora.matmult_a11(m.dims, m.coords, eta, mask, x)
+    with make_op(m, eta, mask) as op:
+        y32 = op.MatMult_MFStokes_A11(torch.from_numpy(x).float().cuda()).double().cpu().numpy()
+        assert relerr(y32, ref) < TOL32
+
+
+def test_unknown_a11_op_rejected(torch_cuda):
+    from pt_b200 import MatStokesMF, PtError
+    with pytest.raises(PtError, match="No -a11_op"):
+        MatStokesMF(2, 2, 2, a11_op="avx")
+
+
+def test_apply_before_setup_is_an_error(torch_cuda):
+    from pt_b200 import MatStokesMF, PtError
+    with MatStokesMF(2, 2, 2) as op:
+        with pytest.raises(PtError, match="PT_ERR_STATE"):
+            op.MFStokesWrapper_A11(np.zeros(op.nvel))
+
+
+def test_large_mesh_properties(torch_cuda, ora):
+    """At 64^3 (6.4M velocity dofs, sinker viscosity): direct oracle
+    comparison plus the size-independent invariants: symmetry of A11,
+    linearity, rigid-body null space, A12 = A21^T."""
+    torch = torch_cuda
+    m, eta, mask = M.problem("c1", seed=0)
+    u = M.uniform_vec(m.nvel, 1)
+    v = M.uniform_vec(m.nvel, 2)
+    p = M.uniform_vec(m.npres, 3)
+    with make_op(m, eta, None) as op:
+        ud, vd = torch.from_numpy(u).cuda(), torch.from_numpy(v).cuda()
+        Au = op.MFStokesWrapper_A11(ud)
+        Av = op.MFStokesWrapper_A11(vd)
+        # symmetry: v.(A u) == u.(A v)
+        a, b = float(torch.dot(vd, Au)), float(torch.dot(ud, Av))
+        assert abs(a - b) <= 1e-12 * (abs(a) + abs(b))
+        # linearity
+        Aw = op.MFStokesWrapper_A11(2.0 * ud - 3.0 * vd)
+        assert relerr(Aw.cpu().numpy(), (2.0 * Au - 3.0 * Av).cpu().numpy()) < 1e-12
+        # rigid rotation about z is in the kernel
+        x = m.coords.reshape(-1, 3)
+        rot = np.cross(np.array([0.0, 0.0, 1.0])[None, :], x).reshape(-1)
+        Ar = op.MFStokesWrapper_A11(torch.from_numpy(rot).cuda())
+        assert float(Ar.abs().max()) < 1e-12 * float(Au.abs().max())
+        # adjointness of B and B^T
+        Bu = op.MFStokesWrapper_A21(ud)
+        Btp = op.MFStokesWrapper_A12(torch.from_numpy(p).cuda())
+        lhs = float(torch.dot(torch.from_numpy(p).cuda(), Bu))
+        rhs = float(torch.dot(Btp, ud))
+        assert abs(lhs - rhs) <= 1e-12 * (abs(lhs) + abs(rhs))
+        # direct comparison with the oracle at this size
+        assert relerr(Au.cpu().numpy(), ora.a11(m.dims, m.coords, eta, u)) < TOL64
