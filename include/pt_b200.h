@@ -3,9 +3,12 @@
  * pTatin3D's matrix-free Q2-P1disc Stokes operator hot path.
  *
  * Plain C types only (no CUDA or PETSc types): pointers, sizes, a status code.
- * Streams are passed as `void *` holding a cudaStream_t (NULL = the op's own
- * stream).  Every entry point returns pt_status and never exits the process
- * (the reference CUDA back-end calls cudaDeviceReset()+exit on errors,
+ * Streams are passed as `void *` holding a cudaStream_t.  An op starts on a
+ * stream of its own; device-pointer (_d) calls are asynchronous on the op's
+ * stream, so a caller whose producers/consumers run on another stream hands
+ * that stream over with pt_op_set_stream (NULL = the legacy default stream).
+ * Every entry point returns pt_status and never exits the process (the
+ * reference CUDA back-end calls cudaDeviceReset()+exit on errors,
  * src/stokes_operators_cuda.cu:46-57).
  *
  * One rank's local problem: on one rank the DMDA ghosted local numbering
@@ -76,7 +79,8 @@ const char *pt_version(void);
 pt_status pt_op_create(const pt_mesh_desc *desc, pt_op **op);
 /* Replaces SpMVOp_Destroy (MFA11Destroy_CUDA, src/stokes_operators_cuda.cu:300-323). */
 pt_status pt_op_destroy(pt_op *op);
-/* Stream for all subsequent work of this op (cudaStream_t as void*). */
+/* Stream for all subsequent work of this op (cudaStream_t as void*; NULL =
+ * the legacy default stream).  Waits for the op's previous stream first. */
 pt_status pt_op_set_stream(pt_op *op, void *stream);
 pt_status pt_op_get_sizes(const pt_op *op, int64_t *nvel, int64_t *npres, int64_t *nel);
 

@@ -297,11 +297,7 @@ pt_status pt_op_set_stream(pt_op *op, void *stream)
   PT_CUDA(cudaStreamSynchronize(op->stream));
   if (op->own_stream) PT_CUDA(cudaStreamDestroy(op->stream));
   op->own_stream = false;
-  op->stream = (cudaStream_t)stream;
-  if (!stream) {
-    PT_CUDA(cudaStreamCreateWithFlags(&op->stream, cudaStreamNonBlocking));
-    op->own_stream = true;
-  }
+  op->stream = (cudaStream_t)stream;  // NULL: the legacy default stream
   return PT_OK;
 }
 

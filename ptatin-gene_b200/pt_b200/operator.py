@@ -61,6 +61,9 @@ class MatStokesMF:
         _capi.call("pt_op_get_sizes", h, ctypes.byref(nv), ctypes.byref(npr), ctypes.byref(nel))
         self.nvel, self.npres, self.nel = nv.value, npr.value, nel.value
         self.set_a11_op(a11_op)
+        if stream is None and torch is not None and torch.cuda.is_available():
+            # order device-pointer calls with torch's work on the current stream
+            stream = torch.cuda.current_stream()
         if stream is not None:
             self.set_stream(stream)
 
@@ -89,6 +92,7 @@ class MatStokesMF:
     def set_stream(self, stream):
         """Use a torch.cuda.Stream (or a raw cudaStream_t int) for all work."""
         raw = stream.cuda_stream if hasattr(stream, "cuda_stream") else int(stream)
+        self.stream = stream
         _capi.call("pt_op_set_stream", self._h, ctypes.c_void_p(raw))
 
     def set_a11_op(self, name: str):
