@@ -62,7 +62,10 @@ typedef enum {
 } pt_status;
 
 typedef struct {
-  int32_t mx, my, mz; /* Q2 elements per axis (>= 1 each) */
+  int32_t mx, my, mz; /* Q2 elements per axis of this rank (>= 1 each) */
+  int32_t nx, ny, nz; /* ghosted local node box; 0 = 2*m+1 (the one-rank box) */
+  int32_t ox, oy, oz; /* node offset of element (0,0,0) in that box: esi-gsi,
+                         esj-gsj, esk-gsk of dmda_element_q2p1.c:395-400 */
 } pt_mesh_desc;
 
 typedef struct pt_op pt_op;
@@ -91,6 +94,10 @@ pt_status pt_op_set_coords_h(pt_op *op, const double *coords);
 pt_status pt_op_set_coords_d(pt_op *op, const double *coords);
 pt_status pt_op_set_eta_h(pt_op *op, const double *eta);
 pt_status pt_op_set_eta_d(pt_op *op, const double *eta);
+/* eta read with a stride (in doubles) between quadrature points: the reference
+ * keeps eta inside the 48-byte QPntVolCoefStokes record, so &qp[0].eta with
+ * stride 6 uploads it without a host-side copy by the caller. */
+pt_status pt_op_set_eta_strided_h(pt_op *op, const double *eta0, int64_t stride);
 pt_status pt_op_set_bc_mask_h(pt_op *op, const uint8_t *mask); /* NULL = no Dirichlet dofs */
 
 /* ---- SpMVOp level ------------------------------------------------------ */

@@ -17,34 +17,41 @@
 
 namespace ptk {
 
+// A rank's element box inside its ghosted local node box.  Element
+// (ei, ej, ek) has node n = a*9 + b*3 + c at
+//   off + (2ei + c) + (2ej + b) X + (2ek + a) XY,   off = ox + oy X + oz XY
+// (the table of src/dmda_element_q2p1.c:395-455 with i = esi-gsi + 2ei).
+struct Box {
+  int mx, my, mz;
+  int64_t X, XY, off;
+};
+
 struct ColourGrid {
-  int mx, my, mz;      // elements per axis
+  Box b;
   int cx, cy, cz;      // colour (parity per axis)
   int ncx, ncy, ncz;   // elements of this colour per axis
 };
 
-__host__ inline ColourGrid colour_grid(int mx, int my, int mz, int colour)
+__host__ inline ColourGrid colour_grid(const Box &b, int colour)
 {
   ColourGrid g;
-  g.mx = mx; g.my = my; g.mz = mz;
+  g.b = b;
   g.cx = colour & 1; g.cy = (colour >> 1) & 1; g.cz = (colour >> 2) & 1;
-  g.ncx = (mx - g.cx + 1) / 2;
-  g.ncy = (my - g.cy + 1) / 2;
-  g.ncz = (mz - g.cz + 1) / 2;
+  g.ncx = (b.mx - g.cx + 1) / 2;
+  g.ncy = (b.my - g.cy + 1) / 2;
+  g.ncz = (b.mz - g.cz + 1) / 2;
   return g;
 }
 
-// Node ids of element (ei, ej, ek): n = a*9 + b*3 + c -> (2ei+c) + (2ej+b)X + (2ek+a)XY.
-__device__ __forceinline__ void element_nodes(int mx, int my, int ei, int ej, int ek, int64_t nid[27])
+__device__ __forceinline__ void element_nodes(const Box &bx, int ei, int ej, int ek, int64_t nid[27])
 {
-  const int64_t X = 2 * (int64_t)mx + 1, XY = X * (2 * (int64_t)my + 1);
-  const int64_t base = 2 * (int64_t)ei + 2 * (int64_t)ej * X + 2 * (int64_t)ek * XY;
+  const int64_t base = bx.off + 2 * (int64_t)ei + 2 * (int64_t)ej * bx.X + 2 * (int64_t)ek * bx.XY;
 #pragma unroll
   for (int a = 0; a < 3; a++)
 #pragma unroll
     for (int b = 0; b < 3; b++)
 #pragma unroll
-      for (int c = 0; c < 3; c++) nid[9 * a + 3 * b + c] = base + c + b * X + a * XY;
+      for (int c = 0; c < 3; c++) nid[9 * a + 3 * b + c] = base + c + b * bx.X + a * bx.XY;
 }
 
 __device__ __forceinline__ bool colour_element(const ColourGrid &g, int64_t t, int &ei, int &ej, int &ek)
@@ -82,9 +89,9 @@ __global__ void __launch_bounds__(128) a11_colour_kernel(ColourGrid g, const T *
 {
   int ei, ej, ek;
   if (!colour_element(g, (int64_t)blockIdx.x * blockDim.x + threadIdx.x, ei, ej, ek)) return;
-  const int64_t e = ei + (int64_t)g.mx * (ej + (int64_t)g.my * ek);
+  const int64_t e = ei + (int64_t)g.b.mx * (ej + (int64_t)g.b.my * ek);
   int64_t nid[27];
-  element_nodes(g.mx, g.my, ei, ej, ek, nid);
+  element_nodes(g.b, ei, ej, ek, nid);
 
   T Jg[3][3][27], Xq[3][27];
   element_jacobian(coords, nid, Jg, Xq);
@@ -146,9 +153,9 @@ __global__ void __launch_bounds__(128) diag_colour_kernel(ColourGrid g, const do
 {
   int ei, ej, ek;
   if (!colour_element(g, (int64_t)blockIdx.x * blockDim.x + threadIdx.x, ei, ej, ek)) return;
-  const int64_t e = ei + (int64_t)g.mx * (ej + (int64_t)g.my * ek);
+  const int64_t e = ei + (int64_t)g.b.mx * (ej + (int64_t)g.b.my * ek);
   int64_t nid[27];
-  element_nodes(g.mx, g.my, ei, ej, ek, nid);
+  element_nodes(g.b, ei, ej, ek, nid);
   double Jg[3][3][27], Xq[3][27];
   element_jacobian(coords, nid, Jg, Xq);
   double acc[27][3];
@@ -209,15 +216,15 @@ __device__ __forceinline__ void p1grel_frame(const double *__restrict__ coords, 
 // No scatter conflicts: one thread writes its own 4 pressure dofs.
 // ---------------------------------------------------------------------------
 template <bool MASKED>
-__global__ void __launch_bounds__(128) a21_kernel(int mx, int my, int mz, const double *__restrict__ coords,
+__global__ void __launch_bounds__(128) a21_kernel(Box bx, const double *__restrict__ coords,
                                                   const double *__restrict__ u, const uint8_t *__restrict__ mask,
                                                   double *__restrict__ yp)
 {
   const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (e >= (int64_t)mx * my * mz) return;
-  const int ei = (int)(e % mx), ej = (int)((e / mx) % my), ek = (int)(e / ((int64_t)mx * my));
+  if (e >= (int64_t)bx.mx * bx.my * bx.mz) return;
+  const int ei = (int)(e % bx.mx), ej = (int)((e / bx.mx) % bx.my), ek = (int)(e / ((int64_t)bx.mx * bx.my));
   int64_t nid[27];
-  element_nodes(mx, my, ei, ej, ek, nid);
+  element_nodes(bx, ei, ej, ek, nid);
   double Jg[3][3][27], Xq[3][27];
   element_jacobian(coords, nid, Jg, Xq);
   double mean[3], invL[3];
@@ -268,9 +275,9 @@ __global__ void __launch_bounds__(128) a12_colour_kernel(ColourGrid g, const dou
 {
   int ei, ej, ek;
   if (!colour_element(g, (int64_t)blockIdx.x * blockDim.x + threadIdx.x, ei, ej, ek)) return;
-  const int64_t e = ei + (int64_t)g.mx * (ej + (int64_t)g.my * ek);
+  const int64_t e = ei + (int64_t)g.b.mx * (ej + (int64_t)g.b.my * ek);
   int64_t nid[27];
-  element_nodes(g.mx, g.my, ei, ej, ek, nid);
+  element_nodes(g.b, ei, ej, ek, nid);
   double Jg[3][3][27], Xq[3][27];
   element_jacobian(coords, nid, Jg, Xq);
   double mean[3], invL[3];

@@ -1,0 +1,346 @@
+// Streaming A11 kernel ("b200"): precomputed quadrature-point geometry,
+// z-marching tiles staged in shared memory, deterministic colour-ordered
+// flushes.
+//
+// Geometry.  At set-up (coordinates or viscosity change) one kernel stores,
+// per element and Gauss point,
+//     K = h * sqrt(c) * adj(J),   c = w * eta / det(J),   h = 1/(2 sqrt(3/5)),
+// nine values.  With A = K Gu' (Gu' = h^-1 d u/d xi, the scaled reference
+// gradient computed below) the viscous action is dv' = (A + A^T) K, which
+// equals h^-1 * w*det*(2 eta sym(grad u)) J^-T of the reference
+// (src/stokes_operators_tensor.c:127-179) -- the scales cancel against the
+// scaled transpose contractions.  The apply therefore reads K instead of
+// coordinates + eta and does no Jacobian work.  c must be > 0 (valid,
+// positively oriented elements and positive viscosity); the op falls back to
+// the 8-colour kernel otherwise.
+//
+// Work decomposition.  A CTA owns TX consecutive elements along x (one
+// thread each) of one element row (ej) and marches over a chunk of LZ element
+// layers in z.  Per layer it holds three node planes of u and of y in shared
+// memory (component-planar, even/odd node split so a warp's 32 elements read
+// consecutive words), computes each element quadrature plane by quadrature
+// plane (the live state is one plane's 3x3 velocity gradient, 81 values), and
+// accumulates the transposed contractions into the y planes.  Within a warp
+// the shared node column of neighbouring elements is updated in program
+// order with a __syncwarp between the i=0 and i=2 passes; the column shared
+// between two warps goes to a per-warp side buffer.  Completed node planes
+// are flushed to global y once.
+//
+// Determinism across CTAs.  Tiles are coloured by the parity of their x-tile,
+// row and z-chunk index; colours run as separate launches in a fixed order.
+// A node on a tile boundary is stored by the first colour that touches it and
+// read-modify-written by the later ones, so every node's sum has a fixed
+// order and no atomics are used.
+#pragma once
+
+#include <cstdint>
+
+#include "kernels_colour.cuh"
+#include "q2_core.cuh"
+#include "q2_plane.cuh"
+
+namespace ptk {
+
+struct StreamGrid {
+  Box b;
+  int TX, ntx;        // elements per tile along x, tiles along x
+  int LZ, nzc;        // layers per z-chunk, z-chunks
+  int px, py, pz;     // colour of this launch
+  int nxc, nyc, nzcc; // tiles of this colour per axis
+  int64_t MXP;        // padded row length of the K array (elements)
+};
+
+// K index: ((row*27 + q)*9 + r)*MXP + ex,  row = ej + my*ek.
+__host__ __device__ __forceinline__ int64_t kidx(int64_t row, int q, int r, int64_t MXP, int ex)
+{
+  return ((row * 27 + q) * 9 + r) * MXP + ex;
+}
+
+// ---------------------------------------------------------------------------
+// Set-up kernel: K for every element and Gauss point.  Returns through
+// *bad the number of points with c <= 0 or non-finite c.
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(128) geom_kernel(Box bx, int64_t MXP, const double *__restrict__ coords,
+                                                   const double *__restrict__ eta, T *__restrict__ K,
+                                                   unsigned int *__restrict__ bad)
+{
+  const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= (int64_t)bx.mx * bx.my * bx.mz) return;
+  const int ei = (int)(e % bx.mx);
+  const int64_t row = e / bx.mx;
+  const int ej = (int)(row % bx.my), ek = (int)(row / bx.my);
+  int64_t nid[27];
+  element_nodes(bx, ei, ej, ek, nid);
+  double Jg[3][3][27], Xq[3][27];
+  element_jacobian(coords, nid, Jg, Xq);
+  unsigned nbad = 0;
+#pragma unroll 1
+  for (int q = 0; q < 27; q++) {
+    double J[3][3];
+#pragma unroll
+    for (int k = 0; k < 3; k++)
+#pragma unroll
+      for (int l = 0; l < 3; l++) J[k][l] = Jg[k][l][q];
+    T Kq[9];
+    if (!q2::geom_K(J, q2::weight(q) * eta[27 * e + q], Kq)) nbad++;
+#pragma unroll
+    for (int r = 0; r < 9; r++) K[kidx(row, q, r, MXP, ei)] = Kq[r];
+  }
+  if (nbad) atomicAdd(bad, nbad);
+}
+
+// Bulk L2 prefetch (TMA unit) of a contiguous K block, in pieces of at most
+// 32 KiB; addresses and sizes are multiples of 16 bytes (MXP is a multiple
+// of 32 elements).
+__device__ __forceinline__ void prefetch_k_plane(const void *p, uint32_t bytes)
+{
+  const char *c = reinterpret_cast<const char *>(p);
+  for (uint32_t off = 0; off < bytes; off += 32768u) {
+    const uint32_t n = min(32768u, bytes - off);
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(c + off), "r"(n) : "memory");
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Shared-memory tile
+// ---------------------------------------------------------------------------
+// Node planes are indexed by slot s = p % 3 (p = absolute node-plane index in
+// the chunk, 2*layer + k).  One plane-row of one component holds the tile's
+// 2TX+1 nodes split even/odd: node 2m -> m, node 2m+1 -> TX+1+m.
+template <int TX>
+struct TileLayout {
+  static constexpr int NXN = 2 * TX + 1;
+  static constexpr int ROW = NXN;              // one (comp, slot, row)
+  static constexpr int PLANE = 3 * ROW;        // 3 rows
+  static constexpr int COMP = 3 * PLANE;       // 3 slots
+  static constexpr int TILE = 3 * COMP;        // 3 components
+  static constexpr int NW = TX / 32;
+  // side buffer: the i=2 column of lane 31 of warps 0..NW-2: [w][slot][row][comp]
+  static constexpr int SIDE = (NW > 1 ? NW - 1 : 1) * 27;
+  __host__ __device__ static constexpr int pos(int n) { return (n & 1) ? (TX + 1 + (n >> 1)) : (n >> 1); }
+  __host__ __device__ static constexpr int at(int comp, int slot, int row, int n)
+  {
+    return comp * COMP + slot * PLANE + row * ROW + pos(n);
+  }
+};
+
+template <typename T, int TX>
+constexpr size_t stream_smem_bytes()
+{
+  using L = TileLayout<TX>;
+  return sizeof(T) * (2 * (size_t)L::TILE + L::SIDE);
+}
+
+// Load node plane p (absolute z node index P) rows 0..2 into slot s.
+template <typename T, int TX, bool MASKED>
+__device__ __forceinline__ void load_plane(T *ut, const StreamGrid &g, int ex0, int ej, int64_t P, int s,
+                                           const T *__restrict__ u, const uint8_t *__restrict__ mask)
+{
+  using L = TileLayout<TX>;
+  const int nvalid = min(L::NXN, 2 * (g.b.mx - ex0) + 1);
+  const int nd = 3 * nvalid;
+#pragma unroll 1
+  for (int r = 0; r < 3; r++) {
+    const int64_t node0 = g.b.off + 2 * (int64_t)ex0 + (2 * (int64_t)ej + r) * g.b.X + P * g.b.XY;
+    const T *src = u + 3 * node0;
+    for (int d = threadIdx.x; d < nd; d += TX) {
+      T v = src[d];
+      if (MASKED && mask[3 * node0 + d]) v = T(0);
+      const int n = d / 3, c = d - 3 * n;
+      ut[L::at(c, s, r, n)] = v;
+    }
+  }
+}
+
+template <typename T, int TX>
+__device__ __forceinline__ void zero_slot(T *yt, T *side, int s)
+{
+  using L = TileLayout<TX>;
+  for (int i = threadIdx.x; i < 3 * L::PLANE; i += TX) {
+    const int c = i / L::PLANE, rest = i - c * L::PLANE;
+    yt[c * L::COMP + s * L::PLANE + rest] = T(0);
+  }
+  for (int i = threadIdx.x; i < (L::NW > 1 ? L::NW - 1 : 0) * 9; i += TX) {
+    const int w = i / 9, rc = i - 9 * w;
+    side[w * 27 + s * 9 + rc] = T(0);
+  }
+}
+
+// Flush node plane P (in slot s) to global y.  zlo/zhi: plane is the chunk's
+// first/last plane and shared with a neighbouring chunk.
+template <typename T, int TX, bool MASKED>
+__device__ __forceinline__ void flush_plane(const T *yt, const T *side, const StreamGrid &g, int tx, int ex0, int ej,
+                                            int64_t P, int s, bool zshared, T *__restrict__ y, const T *__restrict__ x,
+                                            const uint8_t *__restrict__ mask)
+{
+  using L = TileLayout<TX>;
+  const int nvalid = min(L::NXN, 2 * (g.b.mx - ex0) + 1);
+  const bool xlo = tx > 0, xhi = ex0 + TX < g.b.mx;
+  const bool ylo = ej > 0, yhi = ej < g.b.my - 1;
+  const int nd = 3 * nvalid;
+#pragma unroll 1
+  for (int r = 0; r < 3; r++) {
+    const int64_t node0 = g.b.off + 2 * (int64_t)ex0 + (2 * (int64_t)ej + r) * g.b.X + P * g.b.XY;
+    const bool yb = (r == 0 && ylo) || (r == 2 && yhi);
+    for (int d = threadIdx.x; d < nd; d += TX) {
+      const int n = d / 3, c = d - 3 * n;
+      T v = yt[L::at(c, s, r, n)];
+      if (L::NW > 1 && (n & 63) == 0 && n > 0 && n < 2 * TX) v += side[((n >> 6) - 1) * 27 + s * 9 + r * 3 + c];
+      const int64_t k = 3 * node0 + d;
+      if (MASKED && mask[k]) {
+        y[k] = x[k];
+        continue;
+      }
+      const bool xb = (n == 0 && xlo) || (n == 2 * TX && xhi);
+      // stored by the first colour touching the node, added by the later ones
+      const bool first = !((xb && g.px) || (yb && g.py) || (zshared && g.pz));
+      if (first) y[k] = v;
+      else y[k] = y[k] + v;
+    }
+  }
+}
+
+// One element (thread t of the tile), quadrature plane A: forward from the u
+// tile, viscous action with K, transpose accumulated into the y tile.
+template <typename T, int TX, int A>
+__device__ __forceinline__ void element_plane(const T *ut, T *yt, T *side, const int sl[3], int t, int warp,
+                                              bool to_side, unsigned amask, const T *__restrict__ Ke, int64_t MXP)
+{
+  using L = TileLayout<TX>;
+  T G[3][3][9];  // [d][l][b*3+c]
+#pragma unroll
+  for (int l = 0; l < 3; l++) {
+    T Q[9], R[9];
+#pragma unroll
+    for (int j = 0; j < 3; j++)
+#pragma unroll
+      for (int i = 0; i < 3; i++) {
+        const int n = 2 * t + i;
+        q2::zeta_fwd<T, A>(ut[L::at(l, sl[0], j, n)], ut[L::at(l, sl[1], j, n)], ut[L::at(l, sl[2], j, n)],
+                           Q[3 * j + i], R[3 * j + i]);
+      }
+    q2::plane_fwd(Q, R, G[0][l], G[1][l], G[2][l]);
+  }
+
+  // viscous action; K of the next point is loaded while this one computes
+  const T *kp = Ke + (int64_t)(9 * A) * 9 * MXP;
+  T Kn[9];
+#pragma unroll
+  for (int r = 0; r < 9; r++) Kn[r] = kp[(int64_t)r * MXP];
+#pragma unroll
+  for (int p = 0; p < 9; p++) {
+    T Kq[9];
+#pragma unroll
+    for (int r = 0; r < 9; r++) Kq[r] = Kn[r];
+    if (p < 8) {
+#pragma unroll
+      for (int r = 0; r < 9; r++) Kn[r] = kp[(int64_t)(9 * (p + 1) + r) * MXP];
+    }
+    q2::qp_action_K(Kq, G, p);
+  }
+
+  // transpose, one component at a time; node columns i = 0, 1, 2 in order
+#pragma unroll
+  for (int l = 0; l < 3; l++) {
+    T Qt[9], Rt[9];
+    q2::plane_bwd(G[0][l], G[1][l], G[2][l], Qt, Rt);
+#pragma unroll
+    for (int i = 0; i < 3; i++) {
+      if (i == 2) __syncwarp(amask);
+#pragma unroll
+      for (int j = 0; j < 3; j++) {
+        T c0, c1, c2;
+        q2::zeta_bwd<T, A>(Qt[3 * j + i], Rt[3 * j + i], c0, c1, c2);
+        if (i == 2 && to_side) {
+          T *sb = side + warp * 27 + 3 * j + l;
+          sb[sl[0] * 9] += c0;
+          sb[sl[1] * 9] += c1;
+          sb[sl[2] * 9] += c2;
+        } else {
+          const int n = 2 * t + i;
+          yt[L::at(l, sl[0], j, n)] += c0;
+          yt[L::at(l, sl[1], j, n)] += c1;
+          yt[L::at(l, sl[2], j, n)] += c2;
+        }
+      }
+    }
+    __syncwarp(amask);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// The apply kernel
+// ---------------------------------------------------------------------------
+template <typename T, int TX, bool MASKED>
+__global__ void __launch_bounds__(TX, 256 / TX) a11_stream_kernel(StreamGrid g, const T *__restrict__ K,
+                                                                  const T *__restrict__ u,
+                                                                  const uint8_t *__restrict__ mask,
+                                                                  T *__restrict__ y)
+{
+  using L = TileLayout<TX>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T *ut = reinterpret_cast<T *>(smem_raw);
+  T *yt = ut + L::TILE;
+  T *side = yt + L::TILE;
+
+  // tile of this CTA within the colour class
+  const int bid = blockIdx.x;
+  const int ixc = bid % g.nxc, iyc = (bid / g.nxc) % g.nyc, izc = bid / (g.nxc * g.nyc);
+  const int tx = g.px + 2 * ixc, ej = g.py + 2 * iyc, zc = g.pz + 2 * izc;
+  const int ex0 = tx * TX;
+  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+  const int ex = ex0 + t;
+  const bool active = ex < g.b.mx;
+  const int ek0 = zc * g.LZ, ek1 = min(ek0 + g.LZ, g.b.mz);
+  const bool zlo_shared = zc > 0, zhi_shared = ek1 < g.b.mz;
+
+  // prologue: planes 2ek0 .. 2ek0+2 of u, zero y slots
+  for (int k = 0; k < 3; k++) {
+    const int64_t P = 2 * (int64_t)ek0 + k;
+    load_plane<T, TX, MASKED>(ut, g, ex0, ej, P, (int)(P % 3), u, mask);
+    zero_slot<T, TX>(yt, side, (int)(P % 3));
+  }
+  __syncthreads();
+
+  // the node column of a thread's i=2 nodes lives in the side buffer for
+  // lane 31 of every warp but the last
+  const bool to_side = (lane == 31) && (warp < L::NW - 1);
+  const unsigned amask = __ballot_sync(0xffffffffu, active);
+  if (t == 0) prefetch_k_plane(K + kidx(ej + (int64_t)g.b.my * ek0, 0, 0, g.MXP, 0), (uint32_t)(sizeof(T) * 81 * g.MXP));
+
+#pragma unroll 1
+  for (int ek = ek0; ek < ek1; ek++) {
+    const int64_t row = ej + (int64_t)g.b.my * ek;
+    const int s0 = (int)((2 * (int64_t)ek) % 3), s1 = (s0 + 1) % 3, s2 = (s0 + 2) % 3;
+    const int sl[3] = {s0, s1, s2};
+
+    if (active) {
+      const int64_t krow = kidx(row, 0, 0, g.MXP, ex);
+      element_plane<T, TX, 0>(ut, yt, side, sl, t, warp, to_side, amask, K + krow, g.MXP);
+      if (t == 0) prefetch_k_plane(K + kidx(row, 18, 0, g.MXP, 0), (uint32_t)(sizeof(T) * 81 * g.MXP));
+      element_plane<T, TX, 1>(ut, yt, side, sl, t, warp, to_side, amask, K + krow, g.MXP);
+      if (t == 0 && ek + 1 < ek1)
+        prefetch_k_plane(K + kidx(row + g.b.my, 0, 0, g.MXP, 0), (uint32_t)(sizeof(T) * 81 * g.MXP));
+      element_plane<T, TX, 2>(ut, yt, side, sl, t, warp, to_side, amask, K + krow, g.MXP);
+    }
+    __syncthreads();
+
+    // planes 2ek and 2ek+1 are complete for this CTA
+    flush_plane<T, TX, MASKED>(yt, side, g, tx, ex0, ej, 2 * (int64_t)ek, s0, ek == ek0 && zlo_shared, y, u, mask);
+    flush_plane<T, TX, MASKED>(yt, side, g, tx, ex0, ej, 2 * (int64_t)ek + 1, s1, false, y, u, mask);
+    if (ek + 1 == ek1)
+      flush_plane<T, TX, MASKED>(yt, side, g, tx, ex0, ej, 2 * (int64_t)ek + 2, s2, zhi_shared, y, u, mask);
+    __syncthreads();
+    if (ek + 1 < ek1) {
+      // slots s0, s1 take node planes 2ek+3, 2ek+4
+      zero_slot<T, TX>(yt, side, s0);
+      zero_slot<T, TX>(yt, side, s1);
+      load_plane<T, TX, MASKED>(ut, g, ex0, ej, 2 * (int64_t)ek + 3, s0, u, mask);
+      load_plane<T, TX, MASKED>(ut, g, ex0, ej, 2 * (int64_t)ek + 4, s1, u, mask);
+      __syncthreads();
+    }
+  }
+}
+
+}  // namespace ptk

@@ -15,6 +15,7 @@
 
 #include "pt_b200.h"
 #include "kernels_colour.cuh"
+#include "kernels_stream.cuh"
 
 namespace {
 
@@ -53,6 +54,7 @@ enum A11Kernel { A11_STREAM = 0, A11_COLOUR = 1 };
 }  // namespace
 
 struct pt_op {
+  ptk::Box box;
   int mx, my, mz;
   int64_t nnodes, nvel, nel, npres;
   cudaStream_t stream;
@@ -62,6 +64,13 @@ struct pt_op {
   uint8_t *d_mask;
   bool has_coords, has_eta, has_mask;
   double *d_u, *d_y, *d_p; // staging for _h calls
+  // streaming kernel: per-Gauss-point geometry K (FP64 and FP32 copies)
+  double *d_K;
+  float *d_K32;
+  unsigned int *d_bad;
+  int64_t MXP;
+  int TX, ntx, LZ, nzc;
+  bool geom_dirty, geom_ok, full_box;
   int a11_kernel;
   int64_t launches;
   int device;
@@ -137,14 +146,104 @@ pt_status upload_diag_tables()
   return PT_OK;
 }
 
+
+// ---- streaming kernel: geometry set-up and launch -----------------------------
+
+template <typename T, int TX, bool MASKED>
+pt_status launch_stream_tx(pt_op *op, const T *K, const T *u, T *y)
+{
+  constexpr size_t smem = ptk::stream_smem_bytes<T, TX>();
+  static bool attr_set[64] = {false};
+  if (op->device < 64 && !attr_set[op->device]) {
+    PT_CUDA(cudaFuncSetAttribute(ptk::a11_stream_kernel<T, TX, MASKED>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smem));
+    attr_set[op->device] = true;
+  }
+  ptk::StreamGrid g;
+  g.b = op->box;
+  g.TX = TX; g.ntx = op->ntx; g.LZ = op->LZ; g.nzc = op->nzc; g.MXP = op->MXP;
+  for (int pz = 0; pz < 2; pz++)
+    for (int py = 0; py < 2; py++)
+      for (int px = 0; px < 2; px++) {
+        g.px = px; g.py = py; g.pz = pz;
+        g.nxc = (op->ntx - px + 1) / 2;
+        g.nyc = (op->my - py + 1) / 2;
+        g.nzcc = (op->nzc - pz + 1) / 2;
+        const int64_t n = (int64_t)g.nxc * g.nyc * g.nzcc;
+        if (n == 0) continue;
+        ptk::a11_stream_kernel<T, TX, MASKED><<<(unsigned)n, TX, smem, op->stream>>>(g, K, u, MASKED ? op->d_mask : nullptr, y);
+        PT_LAUNCHED(op);
+      }
+  return PT_OK;
+}
+
+template <typename T, bool MASKED>
+pt_status launch_stream(pt_op *op, const T *K, const T *u, T *y)
+{
+  if (op->TX == 32) return launch_stream_tx<T, 32, MASKED>(op, K, u, y);
+  if (op->TX == 64) return launch_stream_tx<T, 64, MASKED>(op, K, u, y);
+  return launch_stream_tx<T, 128, MASKED>(op, K, u, y);
+}
+
+// Recompute K when coordinates or viscosity changed.  Sets geom_ok = false
+// (and the op falls back to the colour kernel) if any c = w eta / det <= 0.
+pt_status ensure_geometry(pt_op *op)
+{
+  if (!op->geom_dirty) return PT_OK;
+  const int64_t nk = (int64_t)op->my * op->mz * 243 * op->MXP;
+  if (!op->d_K) {
+    PT_CUDA(cudaMalloc(&op->d_K, sizeof(double) * nk));
+    PT_CUDA(cudaMalloc(&op->d_K32, sizeof(float) * nk));
+    PT_CUDA(cudaMalloc(&op->d_bad, sizeof(unsigned int)));
+  }
+  PT_CUDA(cudaMemsetAsync(op->d_bad, 0, sizeof(unsigned int), op->stream));
+  ptk::geom_kernel<double><<<nblocks(op->nel), TPB, 0, op->stream>>>(op->box, op->MXP, op->d_coords, op->d_eta,
+                                                                       op->d_K, op->d_bad);
+  PT_LAUNCHED(op);
+  ptk::geom_kernel<float><<<nblocks(op->nel), TPB, 0, op->stream>>>(op->box, op->MXP, op->d_coords, op->d_eta,
+                                                                      op->d_K32, op->d_bad);
+  PT_LAUNCHED(op);
+  unsigned int bad = 0;
+  PT_CUDA(cudaMemcpyAsync(&bad, op->d_bad, sizeof bad, cudaMemcpyDeviceToHost, op->stream));
+  PT_CUDA(cudaStreamSynchronize(op->stream));
+  op->geom_ok = (bad == 0);
+  op->geom_dirty = false;
+  return PT_OK;
+}
+
 // ---- A11 dispatch -----------------------------------------------------------
+
+template <typename T>
+const T *op_K(const pt_op *op);
+template <>
+const double *op_K<double>(const pt_op *op) { return op->d_K; }
+template <>
+const float *op_K<float>(const pt_op *op) { return op->d_K32; }
 
 template <typename T>
 pt_status launch_a11(pt_op *op, const T *coords, const T *eta, const T *u, T *y, bool masked)
 {
+  if (op->a11_kernel == A11_STREAM) {
+    pt_status s = ensure_geometry(op);
+    if (s != PT_OK) return s;
+    if (op->geom_ok) {
+      if (!op->full_box) PT_CUDA(cudaMemsetAsync(y, 0, sizeof(T) * op->nvel, op->stream));
+      if (masked) {
+        if ((s = launch_stream<T, true>(op, op_K<T>(op), u, y)) != PT_OK) return s;
+        // the kernel writes y_k = x_k on Dirichlet dofs inside the element box;
+        // nodes outside it (ghost layers) get the same rule here
+        if (!op->full_box) {
+          bc_copy_kernel<T><<<grid_stride_blocks(op->nvel), 256, 0, op->stream>>>(op->d_mask, u, y, op->nvel);
+          PT_LAUNCHED(op);
+        }
+        return PT_OK;
+      }
+      return launch_stream<T, false>(op, op_K<T>(op), u, y);
+    }
+  }
   PT_CUDA(cudaMemsetAsync(y, 0, sizeof(T) * op->nvel, op->stream));
   for (int c = 0; c < 8; c++) {
-    ptk::ColourGrid g = ptk::colour_grid(op->mx, op->my, op->mz, c);
+    ptk::ColourGrid g = ptk::colour_grid(op->box, c);
     const int64_t n = (int64_t)g.ncx * g.ncy * g.ncz;
     if (n == 0) continue;
     if (masked)
@@ -162,7 +261,7 @@ pt_status diag_d(pt_op *op, double *d)
   if (s != PT_OK) return s;
   PT_CUDA(cudaMemsetAsync(d, 0, sizeof(double) * op->nvel, op->stream));
   for (int c = 0; c < 8; c++) {
-    ptk::ColourGrid g = ptk::colour_grid(op->mx, op->my, op->mz, c);
+    ptk::ColourGrid g = ptk::colour_grid(op->box, c);
     const int64_t n = (int64_t)g.ncx * g.ncy * g.ncz;
     if (n == 0) continue;
     ptk::diag_colour_kernel<<<nblocks(n), TPB, 0, op->stream>>>(g, op->d_coords, op->d_eta, d);
@@ -174,9 +273,9 @@ pt_status diag_d(pt_op *op, double *d)
 pt_status a21_d(pt_op *op, const double *u, double *yp, bool masked)
 {
   if (masked)
-    ptk::a21_kernel<true><<<nblocks(op->nel), TPB, 0, op->stream>>>(op->mx, op->my, op->mz, op->d_coords, u, op->d_mask, yp);
+    ptk::a21_kernel<true><<<nblocks(op->nel), TPB, 0, op->stream>>>(op->box, op->d_coords, u, op->d_mask, yp);
   else
-    ptk::a21_kernel<false><<<nblocks(op->nel), TPB, 0, op->stream>>>(op->mx, op->my, op->mz, op->d_coords, u, nullptr, yp);
+    ptk::a21_kernel<false><<<nblocks(op->nel), TPB, 0, op->stream>>>(op->box, op->d_coords, u, nullptr, yp);
   PT_LAUNCHED(op);
   return PT_OK;
 }
@@ -185,7 +284,7 @@ pt_status a12_d(pt_op *op, const double *p, double *yu)
 {
   PT_CUDA(cudaMemsetAsync(yu, 0, sizeof(double) * op->nvel, op->stream));
   for (int c = 0; c < 8; c++) {
-    ptk::ColourGrid g = ptk::colour_grid(op->mx, op->my, op->mz, c);
+    ptk::ColourGrid g = ptk::colour_grid(op->box, c);
     const int64_t n = (int64_t)g.ncx * g.ncy * g.ncz;
     if (n == 0) continue;
     ptk::a12_colour_kernel<<<nblocks(n), TPB, 0, op->stream>>>(g, op->d_coords, p, yu);
@@ -248,17 +347,41 @@ pt_status pt_op_create(const pt_mesh_desc *desc, pt_op **out)
   *out = nullptr;
   if (desc->mx < 1 || desc->my < 1 || desc->mz < 1)
     return fail(PT_ERR_BAD_ARG, "element counts must be >= 1 (got %d x %d x %d)", desc->mx, desc->my, desc->mz);
-  const int64_t nx = 2 * (int64_t)desc->mx + 1, ny = 2 * (int64_t)desc->my + 1, nz = 2 * (int64_t)desc->mz + 1;
+  const int64_t nx = desc->nx ? desc->nx : 2 * (int64_t)desc->mx + 1;
+  const int64_t ny = desc->ny ? desc->ny : 2 * (int64_t)desc->my + 1;
+  const int64_t nz = desc->nz ? desc->nz : 2 * (int64_t)desc->mz + 1;
+  if (desc->ox < 0 || desc->oy < 0 || desc->oz < 0 || desc->ox + 2 * (int64_t)desc->mx + 1 > nx ||
+      desc->oy + 2 * (int64_t)desc->my + 1 > ny || desc->oz + 2 * (int64_t)desc->mz + 1 > nz)
+    return fail(PT_ERR_BAD_ARG, "element box (%d,%d,%d)+(%d,%d,%d) does not fit the node box %lld x %lld x %lld",
+                desc->ox, desc->oy, desc->oz, desc->mx, desc->my, desc->mz, (long long)nx, (long long)ny, (long long)nz);
   const int64_t nnodes = nx * ny * nz;
   if (nnodes > ((int64_t)1 << 40)) return fail(PT_ERR_BAD_ARG, "mesh too large");
   pt_op *op = (pt_op *)calloc(1, sizeof(pt_op));
   if (!op) return fail(PT_ERR_OOM, "host allocation failed");
   op->mx = desc->mx; op->my = desc->my; op->mz = desc->mz;
+  op->box.mx = desc->mx; op->box.my = desc->my; op->box.mz = desc->mz;
+  op->box.X = nx; op->box.XY = nx * ny;
+  op->box.off = desc->ox + desc->oy * nx + desc->oz * nx * ny;
   op->nnodes = nnodes;
   op->nvel = 3 * nnodes;
   op->nel = (int64_t)desc->mx * desc->my * desc->mz;
   op->npres = 4 * op->nel;
-  op->a11_kernel = A11_COLOUR;
+  op->a11_kernel = A11_STREAM;
+  op->TX = desc->mx <= 32 ? 32 : (desc->mx <= 64 ? 64 : 128);
+  op->ntx = (desc->mx + op->TX - 1) / op->TX;
+  op->MXP = (int64_t)op->ntx * op->TX;
+  {
+    // about 2048 CTAs in total, at least 2 layers per z-chunk where possible
+    const int64_t txy = (int64_t)op->ntx * desc->my;
+    int nzc = (int)((2048 + txy - 1) / txy);
+    nzc = nzc < 1 ? 1 : (nzc > (desc->mz + 1) / 2 ? (desc->mz + 1) / 2 : nzc);
+    if (nzc < 1) nzc = 1;
+    op->LZ = (desc->mz + nzc - 1) / nzc;
+    op->nzc = (desc->mz + op->LZ - 1) / op->LZ;
+  }
+  op->full_box = (nx == 2 * (int64_t)desc->mx + 1) && (ny == 2 * (int64_t)desc->my + 1) &&
+                 (nz == 2 * (int64_t)desc->mz + 1);
+  op->geom_dirty = true;
   cudaError_t e = cudaGetDevice(&op->device);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&op->stream, cudaStreamNonBlocking);
   if (e == cudaSuccess) op->own_stream = true;
@@ -286,6 +409,7 @@ pt_status pt_op_destroy(pt_op *op)
   cudaFree(op->d_coords32); cudaFree(op->d_eta32);
   cudaFree(op->d_mask);
   cudaFree(op->d_u); cudaFree(op->d_y); cudaFree(op->d_p);
+  cudaFree(op->d_K); cudaFree(op->d_K32); cudaFree(op->d_bad);
   if (op->own_stream && op->stream) cudaStreamDestroy(op->stream);
   free(op);
   return PT_OK;
@@ -315,6 +439,7 @@ static pt_status finish_coords(pt_op *op)
   to_f32_kernel<<<grid_stride_blocks(op->nvel), 256, 0, op->stream>>>(op->d_coords, op->d_coords32, op->nvel);
   PT_LAUNCHED(op);
   op->has_coords = true;
+  op->geom_dirty = true;
   return PT_OK;
 }
 
@@ -323,6 +448,7 @@ static pt_status finish_eta(pt_op *op)
   to_f32_kernel<<<grid_stride_blocks(27 * op->nel), 256, 0, op->stream>>>(op->d_eta, op->d_eta32, 27 * op->nel);
   PT_LAUNCHED(op);
   op->has_eta = true;
+  op->geom_dirty = true;
   return PT_OK;
 }
 
@@ -358,6 +484,20 @@ pt_status pt_op_set_eta_d(pt_op *op, const double *eta)
   if (!op || !eta) return fail(PT_ERR_BAD_ARG, "NULL argument");
   PT_CUDA(cudaMemcpyAsync(op->d_eta, eta, sizeof(double) * 27 * op->nel, cudaMemcpyDeviceToDevice, op->stream));
   return finish_eta(op);
+}
+
+pt_status pt_op_set_eta_strided_h(pt_op *op, const double *eta0, int64_t stride)
+{
+  if (!op || !eta0) return fail(PT_ERR_BAD_ARG, "NULL argument");
+  if (stride < 1) return fail(PT_ERR_BAD_ARG, "stride must be >= 1 (got %lld)", (long long)stride);
+  if (stride == 1) return pt_op_set_eta_h(op, eta0);
+  const int64_t n = 27 * op->nel;
+  double *tmp = nullptr;
+  PT_CUDA(cudaMallocHost(&tmp, sizeof(double) * n));
+  for (int64_t i = 0; i < n; i++) tmp[i] = eta0[i * stride];
+  pt_status s = pt_op_set_eta_h(op, tmp);
+  cudaFreeHost(tmp);
+  return s;
 }
 
 pt_status pt_op_set_bc_mask_h(pt_op *op, const uint8_t *mask)
@@ -537,7 +677,7 @@ pt_status pt_matmult_a21_h(pt_op *op, const double *u, double *yp)
 pt_status pt_op_set_a11_kernel(pt_op *op, const char *name)
 {
   if (!op || !name) return fail(PT_ERR_BAD_ARG, "NULL argument");
-  if (!strcmp(name, "b200")) op->a11_kernel = A11_COLOUR;
+  if (!strcmp(name, "b200")) op->a11_kernel = A11_STREAM;
   else if (!strcmp(name, "b200_colour")) op->a11_kernel = A11_COLOUR;
   else return fail(PT_ERR_BAD_ARG, "No -a11_op %s", name);
   return PT_OK;

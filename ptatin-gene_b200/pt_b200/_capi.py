@@ -21,7 +21,9 @@ class PtError(RuntimeError):
 
 
 class MeshDesc(ctypes.Structure):
-    _fields_ = [("mx", ctypes.c_int32), ("my", ctypes.c_int32), ("mz", ctypes.c_int32)]
+    _fields_ = [("mx", ctypes.c_int32), ("my", ctypes.c_int32), ("mz", ctypes.c_int32),
+                ("nx", ctypes.c_int32), ("ny", ctypes.c_int32), ("nz", ctypes.c_int32),
+                ("ox", ctypes.c_int32), ("oy", ctypes.c_int32), ("oz", ctypes.c_int32)]
 
 
 _vp = ctypes.c_void_p
@@ -37,6 +39,7 @@ SIGNATURES = {
     "pt_op_set_coords_d": [_vp, _vp],
     "pt_op_set_eta_h": [_vp, _vp],
     "pt_op_set_eta_d": [_vp, _vp],
+    "pt_op_set_eta_strided_h": [_vp, _vp, ctypes.c_int64],
     "pt_op_set_bc_mask_h": [_vp, _vp],
     "pt_a11_apply_h": [_vp, _vp, _vp],
     "pt_a11_apply_d": [_vp, _vp, _vp],

@@ -20,7 +20,7 @@ def core(tmp_path_factory):
                    check=True)
     lib = ctypes.CDLL(str(out))
     dp = ctypes.POINTER(ctypes.c_double)
-    for f in ("core_a11_f64", "core_a11_f32"):
+    for f in ("core_a11_f64", "core_a11_f32", "core_a11_plane_f64", "core_a11_plane_f32"):
         getattr(lib, f).argtypes = [ctypes.c_int] * 3 + [dp] * 4
     return lib
 
@@ -40,3 +40,27 @@ def test_core_a11_matches_oracle(core, ora, workload):
     y32 = np.zeros(m.nvel)
     core.core_a11_f32(*m.dims, _p(m.coords), _p(eta), _p(u), _p(y32))
     assert relerr(y32, ref) < 5e-5
+
+
+@pytest.mark.parametrize("workload", ["c0", "box:1,1,1", "box:3,2,4"])
+def test_stream_kernel_algorithm_matches_oracle(core, ora, workload):
+    """Per-plane algorithm of the streaming kernel with the precomputed
+    geometry factor K (csrc/q2_plane.cuh)."""
+    m, eta, _ = M.problem(workload)
+    u = M.uniform_vec(m.nvel, 4)
+    ref = ora.a11(m.dims, m.coords, eta, u)
+    y = np.zeros(m.nvel)
+    assert core.core_a11_plane_f64(*m.dims, _p(m.coords), _p(eta), _p(u), _p(y)) == 0
+    assert relerr(y, ref) < 1e-13
+    y32 = np.zeros(m.nvel)
+    assert core.core_a11_plane_f32(*m.dims, _p(m.coords), _p(eta), _p(u), _p(y32)) == 0
+    assert relerr(y32, ref) < 5e-5
+
+
+def test_stream_geometry_flags_nonpositive_viscosity(core):
+    m, eta, _ = M.problem("box:2,2,2")
+    eta = eta.copy()
+    eta[5] = -1.0
+    y = np.zeros(m.nvel)
+    u = M.uniform_vec(m.nvel, 4)
+    assert core.core_a11_plane_f64(*m.dims, _p(m.coords), _p(eta), _p(u), _p(y)) == 1
