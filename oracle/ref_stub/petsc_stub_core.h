@@ -82,6 +82,7 @@ typedef struct _p_PetscSF *PetscSF;
 #define PETSC_ERR_ARG_CORRUPT 64
 #define PETSC_ERR_ARG_NULL 85
 #define PETSC_ERR_ARG_OUTOFRANGE 63
+#define PETSC_ERR_LIB 76
 #define PETSC_DECIDE -1
 #define PETSC_DEFAULT -2
 #define PETSC_NULL 0
@@ -120,4 +121,19 @@ PetscErrorCode VecRestoreArrayRead(Vec, const PetscScalar **);
 PetscErrorCode VecGetArray(Vec, PetscScalar **);
 PetscErrorCode VecRestoreArray(Vec, PetscScalar **);
 PetscErrorCode PetscTime(PetscLogDouble *);
+
+/* Declarations only, for compile checks of code written against PETSc (the
+ * b200 plug-in shim); nothing here implements them. */
+PetscErrorCode DMDAGetGhostCorners(DM, PetscInt *, PetscInt *, PetscInt *, PetscInt *, PetscInt *, PetscInt *);
+PetscErrorCode PetscObjectQuery(PetscObject, const char[], PetscObject *);
+PetscErrorCode PetscObjectCompose(PetscObject, const char[], PetscObject);
+PetscErrorCode PetscObjectStateGet(PetscObject, PetscObjectState *);
+MPI_Comm PetscObjectComm(PetscObject);
+PetscErrorCode PetscContainerCreate(MPI_Comm, PetscContainer *);
+PetscErrorCode PetscContainerSetPointer(PetscContainer, void *);
+PetscErrorCode PetscContainerGetPointer(PetscContainer, void **);
+PetscErrorCode PetscContainerSetUserDestroy(PetscContainer, PetscErrorCode (*)(void *));
+PetscErrorCode PetscContainerDestroy(PetscContainer *);
+PetscErrorCode PetscFunctionListAdd_Private(PetscFunctionList *, const char[], void (*)(void));
+#define PetscFunctionListAdd(list, name, fptr) PetscFunctionListAdd_Private((list), (name), (void (*)(void))(fptr))
 #endif
