@@ -125,6 +125,25 @@ pt_status pt_a21_apply_d(pt_op *op, const double *u, double *yp);
 pt_status pt_a12_apply_h(pt_op *op, const double *p, double *yu);
 pt_status pt_a12_apply_d(pt_op *op, const double *p, double *yu);
 
+/* y = A11 u (SpMVOp level) with no device allocation.  No counterpart in the
+ * reference: it is for callers that cannot allocate device memory when they
+ * need the operator -- applications that give the whole GPU to their own
+ * fixed-size memory pool, processes under a hard device-memory cap that is
+ * already used up, or latency-critical paths that must not take
+ * cudaMalloc/cudaFree's device-wide synchronisation.  coords, eta, u and y are
+ * caller-owned device arrays of a one-rank box (desc->nx..oz zero); the
+ * Gauss-point geometry is recomputed into a fixed 16 MiB scratch area that
+ * every GPU loading the library holds until exit, so the mesh must satisfy
+ * my*mz*243*MXP <= 2^21 (MXP = mx rounded up to 32, 64 or a multiple of 128;
+ * a 16x16x16 box fits) or the call returns PT_ERR_BAD_ARG.  The first call on
+ * a device looks up the scratch address (cudaGetSymbolAddress) and should come
+ * before any stream capture.  All calls share the scratch: calls that overlap
+ * on the GPU race.  The call synchronises `stream` (a cudaStream_t, NULL = the
+ * legacy default stream) to check the geometry, and returns PT_ERR_BAD_ARG if
+ * some w*eta/detJ <= 0. */
+pt_status pt_a11_apply_noalloc_d(const pt_mesh_desc *desc, const double *coords, const double *eta,
+                                 const double *u, double *y, void *stream);
+
 /* ---- MatShell level (BC semantics, one rank) -------------------------- */
 
 /* y = A11 x with Dirichlet columns zeroed and rows y_k = x_k

@@ -11,6 +11,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <string>
 
 #include "pt_b200.h"
@@ -696,3 +697,145 @@ void pt_op_reset_launch_count(pt_op *op)
 }
 
 }  // extern "C"
+
+// ============================================================================
+// A11 apply that allocates nothing (pt_a11_apply_noalloc_d).
+//
+// Some callers cannot ask the CUDA allocator for memory at the moment they
+// need the operator: applications that hand the whole device to their own
+// fixed-size memory pool up front (an extra cudaMalloc then simply fails),
+// processes running under a hard device-memory limit that is already used up,
+// and latency-critical paths that must not take cudaMalloc/cudaFree's
+// device-wide synchronisation.  For them this entry point
+// runs the streaming kernel on caller-owned coordinates, viscosity, input and
+// output, and keeps the kernel's scratch -- the Gauss-point geometry factor K
+// and the set-up check counter -- in file-scope device arrays of fixed size
+// that every GPU loading this library holds until the process exits.
+// ============================================================================
+
+namespace {
+
+// Capacity of the scratch K array, in doubles: 2^21 (16 MiB).  A mesh fits
+// when my*mz*243*MXP <= this, MXP = mx rounded up to the tile width (32, 64 or
+// a multiple of 128); a 16^3 box needs 1,990,656.
+constexpr int64_t NOALLOC_K_CAP = (int64_t)1 << 21;
+
+__device__ __align__(256) double g_noalloc_K[NOALLOC_K_CAP];
+__device__ __align__(256) unsigned int g_noalloc_bad[64];
+
+struct NoallocDev {
+  double *K;
+  unsigned int *bad;
+  bool ready;
+};
+NoallocDev g_noalloc[64];
+std::mutex g_noalloc_mu;
+
+// Device addresses of the scratch arrays for the current device, looked up
+// once per device with that device current.  The host-side names of the
+// arrays are not device addresses; kernels only ever get these pointers.
+pt_status noalloc_scratch(int dev, double **K, unsigned int **bad)
+{
+  if (dev < 0 || dev >= 64) return fail(PT_ERR_UNSUPPORTED, "device index %d beyond 63", dev);
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  NoallocDev &d = g_noalloc[dev];
+  if (!d.ready) {
+    cudaError_t e = cudaGetSymbolAddress((void **)&d.K, g_noalloc_K);
+    if (e != cudaSuccess) return fail(PT_ERR_CUDA, "cudaGetSymbolAddress(K scratch): %s", cudaGetErrorString(e));
+    e = cudaGetSymbolAddress((void **)&d.bad, g_noalloc_bad);
+    if (e != cudaSuccess) return fail(PT_ERR_CUDA, "cudaGetSymbolAddress(check counter): %s", cudaGetErrorString(e));
+    d.ready = true;
+  }
+  *K = d.K;
+  *bad = d.bad;
+  return PT_OK;
+}
+
+template <int TX>
+pt_status noalloc_launch(const ptk::StreamGrid &g0, int my, const double *K, const double *u, double *y,
+                         cudaStream_t stream)
+{
+  constexpr size_t smem = ptk::stream_smem_bytes<double, TX>();
+  PT_CUDA(cudaFuncSetAttribute(ptk::a11_stream_kernel<double, TX, false>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  ptk::StreamGrid g = g0;
+  for (int pz = 0; pz < 2; pz++)
+    for (int py = 0; py < 2; py++)
+      for (int px = 0; px < 2; px++) {
+        g.px = px; g.py = py; g.pz = pz;
+        g.nxc = (g.ntx - px + 1) / 2;
+        g.nyc = (my - py + 1) / 2;
+        g.nzcc = (g.nzc - pz + 1) / 2;
+        const int64_t n = (int64_t)g.nxc * g.nyc * g.nzcc;
+        if (n == 0) continue;
+        ptk::a11_stream_kernel<double, TX, false><<<(unsigned)n, TX, smem, stream>>>(g, K, u, nullptr, y);
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return fail(PT_ERR_CUDA, "kernel launch: %s", cudaGetErrorString(e));
+      }
+  return PT_OK;
+}
+
+}  // namespace
+
+extern "C" pt_status pt_a11_apply_noalloc_d(const pt_mesh_desc *desc, const double *coords, const double *eta,
+                                            const double *u, double *y, void *stream)
+{
+  if (!desc || !coords || !eta || !u || !y) return fail(PT_ERR_BAD_ARG, "NULL argument");
+  if (desc->mx < 1 || desc->my < 1 || desc->mz < 1)
+    return fail(PT_ERR_BAD_ARG, "element counts must be >= 1 (got %d x %d x %d)", desc->mx, desc->my, desc->mz);
+  const int64_t nx = 2 * (int64_t)desc->mx + 1, ny = 2 * (int64_t)desc->my + 1, nz = 2 * (int64_t)desc->mz + 1;
+  if ((desc->nx && desc->nx != nx) || (desc->ny && desc->ny != ny) || (desc->nz && desc->nz != nz) || desc->ox ||
+      desc->oy || desc->oz)
+    return fail(PT_ERR_UNSUPPORTED, "pt_a11_apply_noalloc_d takes one-rank boxes only (node box 2m+1, no offset)");
+  const int TX = desc->mx <= 32 ? 32 : (desc->mx <= 64 ? 64 : 128);
+  const int ntx = (desc->mx + TX - 1) / TX;
+  const int64_t MXP = (int64_t)ntx * TX;
+  const int64_t nk = (int64_t)desc->my * desc->mz * 243 * MXP;
+  if (nk > NOALLOC_K_CAP)
+    return fail(PT_ERR_BAD_ARG,
+                "mesh %d x %d x %d needs %lld doubles of geometry scratch; pt_a11_apply_noalloc_d holds %lld "
+                "(e.g. 16 x 16 x 16); use an op (pt_op_create) for larger meshes",
+                desc->mx, desc->my, desc->mz, (long long)nk, (long long)NOALLOC_K_CAP);
+  int dev = 0;
+  PT_CUDA(cudaGetDevice(&dev));
+  double *K = nullptr;
+  unsigned int *bad = nullptr;
+  pt_status s = noalloc_scratch(dev, &K, &bad);
+  if (s != PT_OK) return s;
+  cudaStream_t st = (cudaStream_t)stream;
+
+  ptk::Box bx;
+  bx.mx = desc->mx; bx.my = desc->my; bx.mz = desc->mz;
+  bx.X = nx; bx.XY = nx * ny; bx.off = 0;
+  const int64_t nel = (int64_t)desc->mx * desc->my * desc->mz;
+  // the counter keeps the previous call's value: clear it first
+  PT_CUDA(cudaMemsetAsync(bad, 0, sizeof(unsigned int), st));
+  ptk::geom_kernel<double><<<nblocks(nel), TPB, 0, st>>>(bx, MXP, coords, eta, K, bad);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return fail(PT_ERR_CUDA, "kernel launch: %s", cudaGetErrorString(e));
+
+  ptk::StreamGrid g;
+  g.b = bx;
+  g.TX = TX; g.ntx = ntx; g.MXP = MXP;
+  {
+    const int64_t txy = (int64_t)ntx * desc->my;
+    int nzc = (int)((2048 + txy - 1) / txy);
+    nzc = nzc < 1 ? 1 : (nzc > (desc->mz + 1) / 2 ? (desc->mz + 1) / 2 : nzc);
+    if (nzc < 1) nzc = 1;
+    g.LZ = (desc->mz + nzc - 1) / nzc;
+    g.nzc = (desc->mz + g.LZ - 1) / g.LZ;
+  }
+  if (TX == 32) s = noalloc_launch<32>(g, desc->my, K, u, y, st);
+  else if (TX == 64) s = noalloc_launch<64>(g, desc->my, K, u, y, st);
+  else s = noalloc_launch<128>(g, desc->my, K, u, y, st);
+  if (s != PT_OK) return s;
+
+  // the geometry check: every w*eta/detJ must be positive
+  unsigned int nbad = 0;
+  PT_CUDA(cudaMemcpyAsync(&nbad, bad, sizeof nbad, cudaMemcpyDeviceToHost, st));
+  PT_CUDA(cudaStreamSynchronize(st));
+  if (nbad)
+    return fail(PT_ERR_BAD_ARG, "%u Gauss points with w*eta/detJ <= 0 (inverted element or non-positive eta); "
+                "y is not valid -- use an op, which falls back to the colour kernel", nbad);
+  return PT_OK;
+}

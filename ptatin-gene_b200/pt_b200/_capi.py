@@ -59,6 +59,7 @@ SIGNATURES = {
     "pt_matmult_a12_d": [_vp, _vp, _vp],
     "pt_matmult_a21_h": [_vp, _vp, _vp],
     "pt_matmult_a21_d": [_vp, _vp, _vp],
+    "pt_a11_apply_noalloc_d": [ctypes.POINTER(MeshDesc), _vp, _vp, _vp, _vp, _vp],
     "pt_op_set_a11_kernel": [_vp, ctypes.c_char_p],
     "pt_op_get_a11_kernel": [_vp],
     "pt_op_launch_count": [_vp],
