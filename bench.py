@@ -331,6 +331,39 @@ def run_ours(args):
     return 0
 
 
+def run_solve(args):
+    """Precision form: A11 u = f with f uniform [-1, 1] on free dofs, FP64
+    outer Krylov to rtol 1e-8, Chebyshev(3)-Jacobi inner in FP64 vs FP32.
+    Prints one JSON line with both solves and the solutions' difference."""
+    import torch
+
+    from pt_b200 import MatStokesMF
+    from pt_b200 import mesh as M
+    from pt_b200.solver import KSPSolveA11
+    torch.cuda.set_device(0)
+    m, eta, mask = M.problem(args.workload, seed=0)
+    f = M.uniform_vec(m.nvel, 11)
+    f[mask.astype(bool)] = 0.0
+    fd = torch.from_numpy(f).cuda()
+    op = MatStokesMF(*m.dims)
+    op.SetUp(m.coords, eta, mask)
+    out = {"mode": "solve", "workload": args.workload, "nvel": m.nvel, "ksp": args.ksp, "rtol": args.rtol}
+    sols = {}
+    for name, fp32 in (("fp64", 0), ("fp32_smoothed", 1)):
+        x = torch.zeros_like(fd)
+        with KSPSolveA11(op, ksp=args.ksp, cheby_fp32=fp32, rtol=args.rtol, max_it=args.max_it,
+                         restart=args.restart) as k:
+            st = k.solve(fd, x)
+        sols[name] = x
+        out[name] = st
+    d = (sols["fp32_smoothed"] - sols["fp64"]).abs().max().item() / sols["fp64"].abs().max().item()
+    out["solution_relerr_fp32_vs_fp64"] = d
+    out["time_to_solution_speedup"] = out["fp64"]["seconds"] / out["fp32_smoothed"]["seconds"]
+    print(json.dumps(out))
+    op.Destroy()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -342,7 +375,14 @@ def main():
     ap.add_argument("--quick", action="store_true", help="headline A11 only")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--mode", default="apply", choices=["apply", "solve"])
+    ap.add_argument("--ksp", default="fgmres")
+    ap.add_argument("--rtol", type=float, default=1e-8)
+    ap.add_argument("--max-it", type=int, default=20000)
+    ap.add_argument("--restart", type=int, default=30)
     args = ap.parse_args()
+    if args.mode == "solve":
+        return run_solve(args)
     if args.impl == "reference":
         return run_reference(args)
     return run_ours(args)

@@ -164,6 +164,51 @@ pt_status pt_matmult_a12_d(pt_op *op, const double *p, double *yu);
 pt_status pt_matmult_a21_h(pt_op *op, const double *u, double *yp);
 pt_status pt_matmult_a21_d(pt_op *op, const double *u, double *yp);
 
+/* ---- Krylov solve of A11 u = f (precision and serving forms) ------------
+ *
+ * The reference solves the viscous block with FGMRES and multigrid whose
+ * smoothers are Chebyshev-Jacobi sweeps on the A11 shell
+ * (src/ptatin_driver_linear_ts.c:559-883; PETSc KSPFGMRES, KSPCHEBYSHEV +
+ * PCJACOBI, eigenvalue window "esteig 0,0.2,0,1.1").  This solves on the fine
+ * level: FP64 outer Krylov (FGMRES or flexible CG) with the FP64
+ * MatShell-level A11, preconditioned by Chebyshev on D^-1 A (D =
+ * MatGetDiagonal) over [emin, emax] * lambda_max(D^-1 A), optionally in FP32
+ * (FP32 vectors, FP32 A11 apply, FP32 D^-1). Dot products are FP64 and
+ * deterministic.  The rhs should be zero on Dirichlet dofs. */
+typedef enum { PT_KSP_FGMRES = 0, PT_KSP_FCG = 1 } pt_ksp_type;
+typedef enum { PT_PC_NONE = 0, PT_PC_JACOBI = 1, PT_PC_CHEBY_JACOBI = 2 } pt_pc_type;
+
+typedef struct {
+  int32_t ksp;          /* pt_ksp_type */
+  int32_t restart;      /* FGMRES restart length */
+  int32_t max_it;       /* outer iterations */
+  double rtol, atol;    /* ||b - A x|| <= max(rtol ||b - A x0||, atol) */
+  int32_t pc;           /* pt_pc_type */
+  int32_t cheby_degree; /* Chebyshev steps per application (degree-1 A11 applies) */
+  int32_t cheby_fp32;   /* 1: the Chebyshev-Jacobi smoother runs in FP32 */
+  double cheby_emin, cheby_emax; /* window, fractions of lambda_max(D^-1 A) */
+  int32_t eig_its;      /* Jacobi-PCG (Lanczos) steps for lambda_max */
+} pt_solve_opts;
+
+typedef struct {
+  int32_t its, converged;
+  double rnorm0, rnorm; /* true FP64 residual norms, initial and final */
+  double lambda_max;    /* estimate of lambda_max(D^-1 A) */
+  int64_t a11_f64, a11_f32; /* A11 applies in each precision */
+  double seconds;       /* wall time of the solve */
+} pt_solve_stats;
+
+typedef struct pt_solver pt_solver;
+
+/* Defaults: FGMRES(30), rtol 1e-8, max_it 10000, Chebyshev(3)-Jacobi in FP32,
+ * window [0.2, 1.1], 20 Lanczos steps. */
+void pt_solve_opts_default(pt_solve_opts *opts);
+/* Allocates the Krylov workspace on the op's device. */
+pt_status pt_solver_create(pt_op *op, const pt_solve_opts *opts, pt_solver **solver);
+/* x holds the initial guess on entry and the solution on return (device arrays). */
+pt_status pt_solver_solve_d(pt_solver *solver, const double *b, double *x, pt_solve_stats *stats);
+pt_status pt_solver_destroy(pt_solver *solver);
+
 /* ---- selection, in the style of -a11_op --------------------------------- */
 
 /* Select the A11 kernel by name, like the reference's -a11_op function list

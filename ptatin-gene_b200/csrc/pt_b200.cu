@@ -12,6 +12,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <mutex>
+#include <new>
 #include <string>
 
 #include "pt_b200.h"
@@ -839,3 +840,5 @@ extern "C" pt_status pt_a11_apply_noalloc_d(const pt_mesh_desc *desc, const doub
                 "y is not valid -- use an op, which falls back to the colour kernel", nbad);
   return PT_OK;
 }
+
+#include "solver_impl.cuh"

@@ -26,6 +26,19 @@ class MeshDesc(ctypes.Structure):
                 ("ox", ctypes.c_int32), ("oy", ctypes.c_int32), ("oz", ctypes.c_int32)]
 
 
+class SolveOpts(ctypes.Structure):
+    _fields_ = [("ksp", ctypes.c_int32), ("restart", ctypes.c_int32), ("max_it", ctypes.c_int32),
+                ("rtol", ctypes.c_double), ("atol", ctypes.c_double), ("pc", ctypes.c_int32),
+                ("cheby_degree", ctypes.c_int32), ("cheby_fp32", ctypes.c_int32),
+                ("cheby_emin", ctypes.c_double), ("cheby_emax", ctypes.c_double), ("eig_its", ctypes.c_int32)]
+
+
+class SolveStats(ctypes.Structure):
+    _fields_ = [("its", ctypes.c_int32), ("converged", ctypes.c_int32), ("rnorm0", ctypes.c_double),
+                ("rnorm", ctypes.c_double), ("lambda_max", ctypes.c_double), ("a11_f64", ctypes.c_int64),
+                ("a11_f32", ctypes.c_int64), ("seconds", ctypes.c_double)]
+
+
 _vp = ctypes.c_void_p
 _i64p = ctypes.POINTER(ctypes.c_int64)
 
@@ -60,6 +73,10 @@ SIGNATURES = {
     "pt_matmult_a21_h": [_vp, _vp, _vp],
     "pt_matmult_a21_d": [_vp, _vp, _vp],
     "pt_a11_apply_noalloc_d": [ctypes.POINTER(MeshDesc), _vp, _vp, _vp, _vp, _vp],
+    "pt_solve_opts_default": [ctypes.POINTER(SolveOpts)],
+    "pt_solver_create": [_vp, ctypes.POINTER(SolveOpts), ctypes.POINTER(_vp)],
+    "pt_solver_solve_d": [_vp, _vp, _vp, ctypes.POINTER(SolveStats)],
+    "pt_solver_destroy": [_vp],
     "pt_op_set_a11_kernel": [_vp, ctypes.c_char_p],
     "pt_op_get_a11_kernel": [_vp],
     "pt_op_launch_count": [_vp],
@@ -73,6 +90,7 @@ _RESTYPES = {
     "pt_op_get_a11_kernel": ctypes.c_char_p,
     "pt_op_launch_count": ctypes.c_int64,
     "pt_op_reset_launch_count": None,
+    "pt_solve_opts_default": None,
 }
 
 _lib = None
