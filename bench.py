@@ -364,6 +364,74 @@ def run_solve(args):
     return 0
 
 
+def batched_problems(n=256, seed=0):
+    """The batched workload: n boxes with axes drawn from {8,12,16,24,32},
+    per-element log-uniform eta with contrast drawn from {1e2,1e4,1e6},
+    nodes perturbed +-0.05h, free-slip box BCs."""
+    from pt_b200 import mesh as M
+    rng = np.random.default_rng(seed)
+    axes = np.array([8, 12, 16, 24, 32])
+    out = []
+    for i in range(n):
+        mx, my, mz = (int(v) for v in rng.choice(axes, size=3))
+        c = float(rng.choice([1e2, 1e4, 1e6]))
+        m = M.make_mesh(mx, my, mz, perturb=0.05, seed=seed * 100003 + i)
+        eta = M.eta_per_element(m, contrast=c, seed=seed * 100003 + i)
+        out.append((m, eta, M.bc_mask_freeslip(mx, my, mz)))
+    return out
+
+
+def run_batched(args):
+    """Batched form: one batched A11 apply over all problems (work-list
+    launches) vs the same problems applied one after another, FP64 and FP32."""
+    import torch
+
+    from pt_b200 import MatStokesMF
+    from pt_b200.batch import BatchA11, autotune_lz
+    torch.cuda.set_device(0)
+    probs = batched_problems(args.nbatch, seed=0)
+    ops, us64 = [], []
+    for i, (m, eta, mask) in enumerate(probs):
+        op = MatStokesMF(*m.dims)
+        op.SetUp(m.coords, eta, mask)
+        ops.append(op)
+        us64.append(torch.from_numpy(M_uniform(m.nvel, 1000 + i)).cuda())
+    ndof = sum(m.nvel for m, _, _ in probs)
+    out = {"mode": "batched", "problems": len(probs), "velocity_dofs": ndof,
+           "elements": int(sum(m.nel for m, _, _ in probs))}
+
+    def timed(fn, k):
+        for _ in range(2):
+            fn()
+        torch.cuda.synchronize()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record()
+        for _ in range(k):
+            fn()
+        ev1.record()
+        ev1.synchronize()
+        return ev0.elapsed_time(ev1) / k
+
+    for prec, us in (("fp64", us64), ("fp32", [u.float() for u in us64])):
+        ys = [torch.empty_like(u) for u in us]
+        best, table = autotune_lz(ops, us, ys)
+        with BatchA11(ops, lz=best if best else None) as b:
+            t_b = timed(lambda: b.apply(us, ys, masked=True), args.steps)
+            launches = b.launches_per_apply
+        t_s = timed(lambda: [op.MatMult_MFStokes_A11(u, y) for op, u, y in zip(ops, us, ys)], max(2, args.steps // 4))
+        out[prec] = {"batched_ms": t_b, "sequential_ms": t_s, "batched_gdofs": ndof / t_b / 1e6,
+                     "sequential_gdofs": ndof / t_s / 1e6, "speedup": t_s / t_b, "launches_per_apply": launches,
+                     "autotune_lz": best, "autotune_ms": table}
+    print(json.dumps(out))
+    for op in ops:
+        op.Destroy()
+    return 0
+
+
+def M_uniform(n, seed):
+    return np.random.default_rng(seed).uniform(-1.0, 1.0, size=n)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -375,7 +443,8 @@ def main():
     ap.add_argument("--quick", action="store_true", help="headline A11 only")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
-    ap.add_argument("--mode", default="apply", choices=["apply", "solve"])
+    ap.add_argument("--mode", default="apply", choices=["apply", "solve", "batched"])
+    ap.add_argument("--nbatch", type=int, default=256)
     ap.add_argument("--ksp", default="fgmres")
     ap.add_argument("--rtol", type=float, default=1e-8)
     ap.add_argument("--max-it", type=int, default=20000)
@@ -383,6 +452,8 @@ def main():
     args = ap.parse_args()
     if args.mode == "solve":
         return run_solve(args)
+    if args.mode == "batched":
+        return run_batched(args)
     if args.impl == "reference":
         return run_reference(args)
     return run_ours(args)

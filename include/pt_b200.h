@@ -209,11 +209,32 @@ pt_status pt_solver_create(pt_op *op, const pt_solve_opts *opts, pt_solver **sol
 pt_status pt_solver_solve_d(pt_solver *solver, const double *b, double *x, pt_solve_stats *stats);
 pt_status pt_solver_destroy(pt_solver *solver);
 
+/* ---- batched A11 over many independent boxes ----------------------------
+ *
+ * No counterpart in the reference (one operator per rank there).  A work-list
+ * over n ops (one-rank boxes, coords and eta set): every (problem, x-tile,
+ * row, z-chunk) tile, grouped by colour and tile width; an apply is one launch
+ * per non-empty class (at most 8 colours x 3 widths) over the concatenated
+ * list, and each problem's result is bitwise what its own apply gives.
+ * lz[i] = element layers per z-chunk for problem i (0 = the op's default);
+ * the autotuner in pt_b200/batch.py picks it. */
+typedef struct pt_batch pt_batch;
+pt_status pt_batch_create(int n, pt_op *const *ops, const int32_t *lz, pt_batch **batch);
+pt_status pt_batch_destroy(pt_batch *batch);
+int64_t pt_batch_launches_per_apply(const pt_batch *batch);
+int64_t pt_batch_tiles(const pt_batch *batch);
+/* y_i = A11_i u_i for every problem; u, y are DEVICE arrays of n device
+ * pointers; masked != 0 gives the MatShell-level BC semantics. */
+pt_status pt_batch_a11_apply_d(pt_batch *batch, const double *const *u, double *const *y, int masked, void *stream);
+pt_status pt_batch_a11_apply_f32_d(pt_batch *batch, const float *const *u, float *const *y, int masked, void *stream);
+
 /* ---- selection, in the style of -a11_op --------------------------------- */
 
 /* Select the A11 kernel by name, like the reference's -a11_op function list
- * (src/stokes_operators.c:123-154).  Names: "b200" (default, the tuned
- * kernel) and "b200_colour" (8-colour element kernel).  Unknown names give
+ * (src/stokes_operators.c:123-154).  Names: "b200" (default, the streaming
+ * kernel with precomputed Gauss-point geometry), "b200_tmem" (its variant with
+ * TMEM accumulators, FP64 rows of 65..128 elements) and "b200_colour"
+ * (8-colour element kernel).  Unknown names give
  * PT_ERR_BAD_ARG, as the reference's SETERRQ1 "No -a11_op %s". */
 pt_status pt_op_set_a11_kernel(pt_op *op, const char *name);
 const char *pt_op_get_a11_kernel(const pt_op *op);

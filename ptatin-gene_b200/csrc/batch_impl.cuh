@@ -1,0 +1,158 @@
+// Batched A11 over many independent one-rank boxes (the batched and served
+// forms).  A pt_batch is a work-list built once from a set of ops: every
+// (problem, x-tile, row, z-chunk) tile of every problem, grouped by colour
+// (parity of x-tile, row and z-chunk) and tile width.  An apply is one launch
+// per non-empty (colour, width) class over the concatenated list -- colours
+// run in a fixed order, so the per-node summation order is the same as a
+// problem's own apply and each result is bitwise the one it gets alone.
+// Included from pt_b200.cu after struct pt_op.
+#pragma once
+
+#include <map>
+#include <vector>
+
+struct pt_batch {
+  int n;
+  std::vector<pt_op *> ops;
+  ptk::BatchProb *d_probs64, *d_probs32;
+  int4 *d_items;
+  struct Cls {
+    int px, py, pz, TX;
+    int64_t off, count;
+  };
+  std::vector<Cls> classes;
+  int64_t tiles;
+};
+
+namespace {
+
+template <typename T, int TX, bool MASKED>
+pt_status batch_launch_cls(const pt_batch *b, const pt_batch::Cls &c, const T *const *u, T *const *y, cudaStream_t st)
+{
+  constexpr size_t smem = ptk::stream_smem_bytes<T, TX>();
+  static bool attr_set[64] = {false};
+  int dev = 0;
+  PT_CUDA(cudaGetDevice(&dev));
+  if (dev < 64 && !attr_set[dev]) {
+    PT_CUDA(cudaFuncSetAttribute(ptk::a11_stream_batch_kernel<T, TX, MASKED>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    attr_set[dev] = true;
+  }
+  const ptk::BatchProb *probs = std::is_same<T, double>::value ? b->d_probs64 : b->d_probs32;
+  ptk::a11_stream_batch_kernel<T, TX, MASKED>
+      <<<(unsigned)c.count, TX, smem, st>>>(probs, b->d_items + c.off, c.px, c.py, c.pz, u, y);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return fail(PT_ERR_CUDA, "batched kernel launch: %s", cudaGetErrorString(e));
+  return PT_OK;
+}
+
+template <typename T, bool MASKED>
+pt_status batch_apply(pt_batch *b, const T *const *u, T *const *y, void *stream)
+{
+  if (!b || !u || !y) return fail(PT_ERR_BAD_ARG, "NULL argument");
+  const cudaStream_t st = (cudaStream_t)stream;
+  for (const pt_batch::Cls &c : b->classes) {
+    pt_status s;
+    if (c.TX == 32) s = batch_launch_cls<T, 32, MASKED>(b, c, u, y, st);
+    else if (c.TX == 64) s = batch_launch_cls<T, 64, MASKED>(b, c, u, y, st);
+    else s = batch_launch_cls<T, 128, MASKED>(b, c, u, y, st);
+    if (s != PT_OK) return s;
+  }
+  return PT_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+pt_status pt_batch_create(int n, pt_op *const *ops, const int32_t *lz, pt_batch **out)
+{
+  if (!out || n < 1 || !ops) return fail(PT_ERR_BAD_ARG, "need n >= 1 ops");
+  *out = nullptr;
+  std::vector<ptk::BatchProb> p64(n), p32(n);
+  // class key: (pass, TX) -> items
+  std::map<std::pair<int, int>, std::vector<int4>> cls;
+  int64_t tiles = 0;
+  for (int i = 0; i < n; i++) {
+    pt_op *op = ops[i];
+    pt_status s = check_ready(op, true);
+    if (s != PT_OK) return s;
+    if (!op->full_box) return fail(PT_ERR_UNSUPPORTED, "batch problem %d: one-rank boxes only", i);
+    if ((s = ensure_geometry(op)) != PT_OK) return s;
+    if (!op->geom_ok) return fail(PT_ERR_BAD_ARG, "batch problem %d has w*eta/detJ <= 0 somewhere", i);
+    ptk::BatchProb d;
+    d.b = op->box;
+    d.ntx = op->ntx;
+    d.MXP = op->MXP;
+    int L = (lz && lz[i] > 0) ? lz[i] : op->LZ;
+    if (L > op->mz) L = op->mz;
+    d.LZ = L;
+    d.nzc = (op->mz + L - 1) / L;
+    d.mask = op->has_mask ? op->d_mask : nullptr;
+    d.K = op->d_K;
+    p64[i] = d;
+    d.K = op->d_K32;
+    p32[i] = d;
+    for (int zc = 0; zc < d.nzc; zc++)
+      for (int ej = 0; ej < op->my; ej++)
+        for (int tx = 0; tx < d.ntx; tx++) {
+          const int pass = (tx & 1) + 2 * (ej & 1) + 4 * (zc & 1);
+          cls[{pass, op->TX}].push_back(make_int4(i, tx, ej, zc));
+          tiles++;
+        }
+  }
+  pt_batch *b = new (std::nothrow) pt_batch();
+  if (!b) return fail(PT_ERR_OOM, "host allocation failed");
+  b->n = n;
+  b->ops.assign(ops, ops + n);
+  b->tiles = tiles;
+  std::vector<int4> all;
+  for (auto &kv : cls) {
+    pt_batch::Cls c;
+    c.px = kv.first.first & 1; c.py = (kv.first.first >> 1) & 1; c.pz = (kv.first.first >> 2) & 1;
+    c.TX = kv.first.second;
+    c.off = (int64_t)all.size();
+    c.count = (int64_t)kv.second.size();
+    all.insert(all.end(), kv.second.begin(), kv.second.end());
+    b->classes.push_back(c);
+  }
+  cudaError_t e = cudaMalloc(&b->d_probs64, sizeof(ptk::BatchProb) * n);
+  if (e == cudaSuccess) e = cudaMalloc(&b->d_probs32, sizeof(ptk::BatchProb) * n);
+  if (e == cudaSuccess) e = cudaMalloc(&b->d_items, sizeof(int4) * all.size());
+  if (e == cudaSuccess) e = cudaMemcpy(b->d_probs64, p64.data(), sizeof(ptk::BatchProb) * n, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(b->d_probs32, p32.data(), sizeof(ptk::BatchProb) * n, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(b->d_items, all.data(), sizeof(int4) * all.size(), cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) {
+    pt_status s = fail(e == cudaErrorMemoryAllocation ? PT_ERR_OOM : PT_ERR_CUDA, "pt_batch_create: %s",
+                       cudaGetErrorString(e));
+    pt_batch_destroy(b);
+    return s;
+  }
+  *out = b;
+  return PT_OK;
+}
+
+pt_status pt_batch_destroy(pt_batch *b)
+{
+  if (!b) return PT_OK;
+  cudaFree(b->d_probs64);
+  cudaFree(b->d_probs32);
+  cudaFree(b->d_items);
+  delete b;
+  return PT_OK;
+}
+
+int64_t pt_batch_launches_per_apply(const pt_batch *b) { return b ? (int64_t)b->classes.size() : 0; }
+int64_t pt_batch_tiles(const pt_batch *b) { return b ? b->tiles : 0; }
+
+pt_status pt_batch_a11_apply_d(pt_batch *b, const double *const *u, double *const *y, int masked, void *stream)
+{
+  return masked ? batch_apply<double, true>(b, u, y, stream) : batch_apply<double, false>(b, u, y, stream);
+}
+
+pt_status pt_batch_a11_apply_f32_d(pt_batch *b, const float *const *u, float *const *y, int masked, void *stream)
+{
+  return masked ? batch_apply<float, true>(b, u, y, stream) : batch_apply<float, false>(b, u, y, stream);
+}
+
+}  // extern "C"

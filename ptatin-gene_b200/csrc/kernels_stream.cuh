@@ -272,22 +272,17 @@ __device__ __forceinline__ void element_plane(const T *ut, T *yt, T *side, const
 // ---------------------------------------------------------------------------
 // The apply kernel
 // ---------------------------------------------------------------------------
+// One tile (x-tile tx, row ej, z-chunk zc) of one problem; the whole CTA.
 template <typename T, int TX, bool MASKED>
-__global__ void __launch_bounds__(TX, 256 / TX) a11_stream_kernel(StreamGrid g, const T *__restrict__ K,
-                                                                  const T *__restrict__ u,
-                                                                  const uint8_t *__restrict__ mask,
-                                                                  T *__restrict__ y)
+__device__ __forceinline__ void stream_tile(const StreamGrid &g, int tx, int ej, int zc, const T *__restrict__ K,
+                                            const T *__restrict__ u, const uint8_t *__restrict__ mask,
+                                            T *__restrict__ y)
 {
   using L = TileLayout<TX>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T *ut = reinterpret_cast<T *>(smem_raw);
   T *yt = ut + L::TILE;
   T *side = yt + L::TILE;
-
-  // tile of this CTA within the colour class
-  const int bid = blockIdx.x;
-  const int ixc = bid % g.nxc, iyc = (bid / g.nxc) % g.nyc, izc = bid / (g.nxc * g.nyc);
-  const int tx = g.px + 2 * ixc, ej = g.py + 2 * iyc, zc = g.pz + 2 * izc;
   const int ex0 = tx * TX;
   const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
   const int ex = ex0 + t;
@@ -341,6 +336,49 @@ __global__ void __launch_bounds__(TX, 256 / TX) a11_stream_kernel(StreamGrid g, 
       __syncthreads();
     }
   }
+}
+
+template <typename T, int TX, bool MASKED>
+__global__ void __launch_bounds__(TX, 256 / TX) a11_stream_kernel(StreamGrid g, const T *__restrict__ K,
+                                                                  const T *__restrict__ u,
+                                                                  const uint8_t *__restrict__ mask,
+                                                                  T *__restrict__ y)
+{
+  // tile of this CTA within the colour class
+  const int bid = blockIdx.x;
+  const int ixc = bid % g.nxc, iyc = (bid / g.nxc) % g.nyc, izc = bid / (g.nxc * g.nyc);
+  stream_tile<T, TX, MASKED>(g, g.px + 2 * ixc, g.py + 2 * iyc, g.pz + 2 * izc, K, u, mask, y);
+}
+
+// ---------------------------------------------------------------------------
+// Batched form: one launch per (colour, tile width) over the concatenated
+// work-list of many independent problems.  A work item is (problem, x-tile,
+// row, z-chunk) of that colour; the problem descriptor carries its box, its
+// tiling and its K; the vector pointers come from per-problem tables.
+// ---------------------------------------------------------------------------
+struct BatchProb {
+  Box b;
+  int ntx, LZ, nzc;
+  int64_t MXP;
+  const void *K;          // T* of the problem's Gauss-point factor
+  const uint8_t *mask;    // Dirichlet mask (MatShell level) or null
+};
+
+template <typename T, int TX, bool MASKED>
+__global__ void __launch_bounds__(TX, 256 / TX) a11_stream_batch_kernel(const BatchProb *__restrict__ probs,
+                                                                        const int4 *__restrict__ items, int px, int py,
+                                                                        int pz, const T *const *__restrict__ uptr,
+                                                                        T *const *__restrict__ yptr)
+{
+  const int4 it = items[blockIdx.x];  // (problem, tx, ej, zc)
+  const BatchProb p = probs[it.x];
+  StreamGrid g;
+  g.b = p.b;
+  g.TX = TX; g.ntx = p.ntx; g.LZ = p.LZ; g.nzc = p.nzc; g.MXP = p.MXP;
+  g.px = px; g.py = py; g.pz = pz;
+  g.nxc = g.nyc = g.nzcc = 0;
+  stream_tile<T, TX, MASKED>(g, it.y, it.z, it.w, reinterpret_cast<const T *>(p.K), uptr[it.x],
+                             MASKED ? p.mask : nullptr, yptr[it.x]);
 }
 
 }  // namespace ptk

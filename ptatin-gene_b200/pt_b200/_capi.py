@@ -77,6 +77,12 @@ SIGNATURES = {
     "pt_solver_create": [_vp, ctypes.POINTER(SolveOpts), ctypes.POINTER(_vp)],
     "pt_solver_solve_d": [_vp, _vp, _vp, ctypes.POINTER(SolveStats)],
     "pt_solver_destroy": [_vp],
+    "pt_batch_create": [ctypes.c_int, _vp, _vp, ctypes.POINTER(_vp)],
+    "pt_batch_destroy": [_vp],
+    "pt_batch_launches_per_apply": [_vp],
+    "pt_batch_tiles": [_vp],
+    "pt_batch_a11_apply_d": [_vp, _vp, _vp, ctypes.c_int, _vp],
+    "pt_batch_a11_apply_f32_d": [_vp, _vp, _vp, ctypes.c_int, _vp],
     "pt_op_set_a11_kernel": [_vp, ctypes.c_char_p],
     "pt_op_get_a11_kernel": [_vp],
     "pt_op_launch_count": [_vp],
@@ -91,6 +97,8 @@ _RESTYPES = {
     "pt_op_launch_count": ctypes.c_int64,
     "pt_op_reset_launch_count": None,
     "pt_solve_opts_default": None,
+    "pt_batch_launches_per_apply": ctypes.c_int64,
+    "pt_batch_tiles": ctypes.c_int64,
 }
 
 _lib = None

@@ -51,7 +51,7 @@ def test_spmvop_level_matches_reference(torch_cuda, name, a11_op):
 # (x-colouring), single rows, many z-chunks (z-colouring)
 @pytest.mark.parametrize("workload", ["c0", "box:3,2,4", "box:1,1,1", "box:1,2,3", "box:7,5,3", "box:33,2,2",
                                       "box:2,40,1", "box:64,3,1", "box:130,2,3", "box:257,1,2", "box:3,2,40",
-                                      "box:65,9,7"])
+                                      "box:65,9,7", "box:128,3,5", "box:100,4,11"])
 def test_matshell_level_matches_oracle(torch_cuda, ora, workload):
     m, eta, mask = M.problem(workload, seed=5)
     x = M.uniform_vec(m.nvel, 6)
@@ -91,13 +91,15 @@ def test_apply_is_deterministic(torch_cuda):
         assert torch.equal(y1, y2)
 
 
-@pytest.mark.parametrize("workload", ["box:40,7,5", "box:150,3,9"])
-def test_kernels_agree(torch_cuda, workload):
-    """The tuned and the 8-colour A11 kernels agree to FP64 rounding."""
+@pytest.mark.parametrize("other", ["b200_colour", "b200_tmem"])
+@pytest.mark.parametrize("workload", ["box:40,7,5", "box:150,3,9", "box:128,4,6"])
+def test_kernels_agree(torch_cuda, workload, other):
+    """The default streaming kernel, its TMEM-accumulator variant (rows of
+    65..128 elements) and the 8-colour kernel agree to FP64 rounding."""
     torch = torch_cuda
     m, eta, mask = M.problem(workload, seed=8)
     xd = torch.from_numpy(M.uniform_vec(m.nvel, 9)).cuda()
-    with make_op(m, eta, mask, "b200") as a, make_op(m, eta, mask, "b200_colour") as b:
+    with make_op(m, eta, mask, "b200") as a, make_op(m, eta, mask, other) as b:
         ya = a.MatMult_MFStokes_A11(xd).cpu().numpy()
         yb = b.MatMult_MFStokes_A11(xd).cpu().numpy()
         assert relerr(ya, yb) < 1e-14
