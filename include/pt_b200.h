@@ -174,9 +174,17 @@ pt_status pt_matmult_a21_d(pt_op *op, const double *u, double *yp);
  * MatShell-level A11, preconditioned by Chebyshev on D^-1 A (D =
  * MatGetDiagonal) over [emin, emax] * lambda_max(D^-1 A), optionally in FP32
  * (FP32 vectors, FP32 A11 apply, FP32 D^-1). Dot products are FP64 and
- * deterministic.  The rhs should be zero on Dirichlet dofs. */
+ * deterministic.  The rhs should be zero on Dirichlet dofs.
+ *
+ * PT_PC_MG is the reference's preconditioner structure: a geometric V-cycle
+ * over nested Q2 levels (coordinates injected as DMDARestrictCoordinates-
+ * Hierarchy does, Gauss-point eta projected, A11 re-discretised on each level
+ * with these kernels, src/ptatin_driver_linear_ts.c:482-514, 674-712), Q2
+ * interpolation / its transpose between levels, Chebyshev(cheby_degree)-Jacobi
+ * pre- and post-smoothing (FP32 when cheby_fp32) and mg_coarse_degree
+ * Chebyshev steps on the coarsest level. */
 typedef enum { PT_KSP_FGMRES = 0, PT_KSP_FCG = 1 } pt_ksp_type;
-typedef enum { PT_PC_NONE = 0, PT_PC_JACOBI = 1, PT_PC_CHEBY_JACOBI = 2 } pt_pc_type;
+typedef enum { PT_PC_NONE = 0, PT_PC_JACOBI = 1, PT_PC_CHEBY_JACOBI = 2, PT_PC_MG = 3 } pt_pc_type;
 
 typedef struct {
   int32_t ksp;          /* pt_ksp_type */
@@ -188,6 +196,12 @@ typedef struct {
   int32_t cheby_fp32;   /* 1: the Chebyshev-Jacobi smoother runs in FP32 */
   double cheby_emin, cheby_emax; /* window, fractions of lambda_max(D^-1 A) */
   int32_t eig_its;      /* Jacobi-PCG (Lanczos) steps for lambda_max */
+  int32_t mg_levels;    /* PT_PC_MG: levels (0 = coarsen while every axis is even and >= 4) */
+  int32_t mg_coarse_degree; /* PT_PC_MG: Chebyshev steps on the coarsest level */
+  int32_t pc_graph;     /* PT_PC_MG: replay the V-cycle as one captured CUDA graph */
+  int32_t mg_assembled; /* PT_PC_MG: levels of <= 32^3 elements keep element matrices and a
+                           coarsest level of <= 1200 dofs is solved by a dense inverse (1),
+                           or every level runs the matrix-free kernels (0) */
 } pt_solve_opts;
 
 typedef struct {
@@ -196,6 +210,10 @@ typedef struct {
   double lambda_max;    /* estimate of lambda_max(D^-1 A) */
   int64_t a11_f64, a11_f32; /* A11 applies in each precision */
   double seconds;       /* wall time of the solve */
+  int32_t mg_levels;    /* PT_PC_MG: levels in the hierarchy (0 otherwise) */
+  int32_t reserved;
+  double a11_coarse;    /* PT_PC_MG: coarse-level A11 applies, counted in fine-apply
+                           units (each weighted by its elements / fine elements) */
 } pt_solve_stats;
 
 typedef struct pt_solver pt_solver;
@@ -207,6 +225,10 @@ void pt_solve_opts_default(pt_solve_opts *opts);
 pt_status pt_solver_create(pt_op *op, const pt_solve_opts *opts, pt_solver **solver);
 /* x holds the initial guess on entry and the solution on return (device arrays). */
 pt_status pt_solver_solve_d(pt_solver *solver, const double *b, double *x, pt_solve_stats *stats);
+/* z = P r with the configured preconditioner (PCApply); sets it up first if
+ * needed (PCSetUp, redone after the op's coordinates, viscosity or mask
+ * change).  Device arrays, FP64. */
+pt_status pt_solver_apply_pc_d(pt_solver *solver, const double *r, double *z);
 pt_status pt_solver_destroy(pt_solver *solver);
 
 /* ---- batched A11 over many independent boxes ----------------------------

@@ -77,6 +77,7 @@ struct pt_op {
   bool geom_dirty, geom_ok, full_box;
   int a11_kernel;
   int64_t launches;
+  uint64_t state;  // bumped whenever coordinates, viscosity or the mask change
   int device;
 };
 
@@ -258,6 +259,13 @@ pt_status ensure_geometry(pt_op *op)
 }
 
 // ---- A11 dispatch -----------------------------------------------------------
+
+// The streaming kernels write y_k = x_k on Dirichlet dofs themselves (and
+// launch_a11 does it for ghost nodes), so MatMult needs no separate pass.
+bool a11_sets_bc_rows(const pt_op *op)
+{
+  return (op->a11_kernel == A11_STREAM || op->a11_kernel == A11_TMEM) && op->geom_ok && !op->geom_dirty;
+}
 
 template <typename T>
 const T *op_K(const pt_op *op);
@@ -486,6 +494,7 @@ static pt_status finish_coords(pt_op *op)
   PT_LAUNCHED(op);
   op->has_coords = true;
   op->geom_dirty = true;
+  op->state++;
   return PT_OK;
 }
 
@@ -495,6 +504,7 @@ static pt_status finish_eta(pt_op *op)
   PT_LAUNCHED(op);
   op->has_eta = true;
   op->geom_dirty = true;
+  op->state++;
   return PT_OK;
 }
 
@@ -552,9 +562,11 @@ pt_status pt_op_set_bc_mask_h(pt_op *op, const uint8_t *mask)
   if (!mask) {
     PT_CUDA(cudaMemsetAsync(op->d_mask, 0, op->nvel, op->stream));
     op->has_mask = false;
+    op->state++;
   } else {
     PT_CUDA(cudaMemcpyAsync(op->d_mask, mask, op->nvel, cudaMemcpyHostToDevice, op->stream));
     op->has_mask = true;
+    op->state++;
   }
   PT_CUDA(cudaStreamSynchronize(op->stream));
   return PT_OK;
@@ -652,6 +664,7 @@ pt_status pt_matmult_a11_d(pt_op *op, const double *x, double *y)
   if (!x || !y) return fail(PT_ERR_BAD_ARG, "NULL vector");
   if (x == y) return fail(PT_ERR_BAD_ARG, "x and y must not alias");
   if ((s = launch_a11<double>(op, op->d_coords, op->d_eta, x, y, op->has_mask)) != PT_OK) return s;
+  if (a11_sets_bc_rows(op)) return PT_OK;
   return bc_copy(op, x, y);
 }
 
@@ -671,6 +684,7 @@ pt_status pt_matmult_a11_f32_d(pt_op *op, const float *x, float *y)
   if (!x || !y) return fail(PT_ERR_BAD_ARG, "NULL vector");
   if (x == y) return fail(PT_ERR_BAD_ARG, "x and y must not alias");
   if ((s = launch_a11<float>(op, op->d_coords32, op->d_eta32, x, y, op->has_mask)) != PT_OK) return s;
+  if (a11_sets_bc_rows(op)) return PT_OK;
   return bc_copy32(op, x, y);
 }
 

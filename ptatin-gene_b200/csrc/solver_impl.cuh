@@ -205,6 +205,8 @@ double tridiag_lambda_max(const std::vector<double> &a, const std::vector<double
 
 }  // namespace
 
+#include "mg_impl.cuh"
+
 struct pt_solver {
   pt_op *op;
   pt_solve_opts o;
@@ -221,17 +223,21 @@ struct pt_solver {
   double lambda_max;
   bool have_diag;
   int64_t n64, n32;
+  pt_mg *mg;
+  bool setup_done;
+  uint64_t op_state;  // op->state the set-up was made for
 };
 
 namespace {
 
-pt_status sv_dots(pt_solver *s, const double *const *vecs_host, int nv, const double *w, double *out)
+pt_status sv_dots(pt_solver *s, const double *const *vecs_host, int nv, const double *w, double *out, int64_t n = -1)
 {
+  if (n < 0) n = s->n;
   // vector-pointer table goes through a small device array
   for (int base = 0; base < nv; base += MDOT_CHUNK) {
     const int k = std::min(MDOT_CHUNK, nv - base);
     PT_CUDA(cudaMemcpyAsync(s->dptr, vecs_host + base, sizeof(double *) * k, cudaMemcpyHostToDevice, s->op->stream));
-    mdot_partial_kernel<<<RED_BLOCKS, RED_THREADS, 0, s->op->stream>>>(s->dptr, k, w, s->n, s->partial);
+    mdot_partial_kernel<<<RED_BLOCKS, RED_THREADS, 0, s->op->stream>>>(s->dptr, k, w, n, s->partial);
     PT_LAUNCHED(s->op);
     mdot_final_kernel<<<1, RED_THREADS, 0, s->op->stream>>>(s->partial, k, s->dres + base);
     PT_LAUNCHED(s->op);
@@ -242,10 +248,10 @@ pt_status sv_dots(pt_solver *s, const double *const *vecs_host, int nv, const do
   return PT_OK;
 }
 
-pt_status sv_dot(pt_solver *s, const double *a, const double *b, double *out)
+pt_status sv_dot(pt_solver *s, const double *a, const double *b, double *out, int64_t n = -1)
 {
   const double *v[1] = {a};
-  return sv_dots(s, v, 1, b, out);
+  return sv_dots(s, v, 1, b, out, n);
 }
 
 // w -= sum h_j v_j  (sign = -1) or x += sum h_j z_j (sign = +1)
@@ -265,9 +271,10 @@ pt_status sv_maxpy(pt_solver *s, const double *const *vecs_host, const double *h
 }
 
 template <typename T>
-pt_status sv_axpby(pt_solver *s, T a, const T *x, T b, T *y)
+pt_status sv_axpby(pt_solver *s, T a, const T *x, T b, T *y, int64_t n = -1)
 {
-  axpby_kernel<T><<<vgrid(s->n), 256, 0, s->op->stream>>>(a, x, b, y, s->n);
+  if (n < 0) n = s->n;
+  axpby_kernel<T><<<vgrid(n), 256, 0, s->op->stream>>>(a, x, b, y, n);
   PT_LAUNCHED(s->op);
   return PT_OK;
 }
@@ -295,33 +302,36 @@ pt_status sv_setup_diag(pt_solver *s)
   return PT_OK;
 }
 
-// lambda_max(D^-1 A) from eig_its steps of Jacobi-PCG on a pseudo-random rhs (Lanczos tridiagonal).
-pt_status sv_estimate_lambda(pt_solver *s)
+// lambda_max(D^-1 A) of operator `op` (n dofs, inverse diagonal dinv) from
+// eig_its steps of Jacobi-PCG on a pseudo-random rhs (Lanczos tridiagonal).
+// Uses the solver's FP64 work vectors (fine-level size >= n).
+pt_status sv_lanczos(pt_solver *s, pt_op *op, int64_t n, const double *dinv, double *lmax)
 {
-  double *b = s->t2, *x = s->x0, *p = s->t3, *q = s->w, *r = s->r, *z = s->t1;
-  hash_vec_kernel<<<vgrid(s->n), 256, 0, s->op->stream>>>(b, s->n, 12345u);
+  double *b = s->t2, *p = s->t3, *q = s->w, *r = s->r, *z = s->t1;
+  cudaStream_t st = s->op->stream;
+  hash_vec_kernel<<<vgrid(n), 256, 0, st>>>(b, n, 12345u);
   PT_LAUNCHED(s->op);
-  PT_CUDA(cudaMemcpyAsync(r, b, sizeof(double) * s->n, cudaMemcpyDeviceToDevice, s->op->stream));
-  PT_CUDA(cudaMemsetAsync(x, 0, sizeof(double) * s->n, s->op->stream));
-  cheb_first_kernel<double><<<vgrid(s->n), 256, 0, s->op->stream>>>(1.0, s->dinv, r, z, p, s->n);  // z = p = D^-1 r
+  PT_CUDA(cudaMemcpyAsync(r, b, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+  cheb_first_kernel<double><<<vgrid(n), 256, 0, st>>>(1.0, dinv, r, z, p, n);  // z = p = D^-1 r
   PT_LAUNCHED(s->op);
   double rz;
-  pt_status st = sv_dot(s, r, z, &rz);
-  if (st != PT_OK) return st;
+  pt_status stt = sv_dot(s, r, z, &rz, n);
+  if (stt != PT_OK) return stt;
   std::vector<double> alphas, betas, diag, off;
   for (int k = 0; k < s->o.eig_its && rz > 0.0; k++) {
-    if ((st = sv_matmult64(s, p, q)) != PT_OK) return st;
+    if (op == s->op) s->n64++;
+    if ((stt = pt_matmult_a11_d(op, p, q)) != PT_OK) return stt;
     double pq;
-    if ((st = sv_dot(s, p, q, &pq)) != PT_OK) return st;
+    if ((stt = sv_dot(s, p, q, &pq, n)) != PT_OK) return stt;
     if (!(pq > 0.0)) break;
     const double alpha = rz / pq;
-    if ((st = sv_axpby<double>(s, -alpha, q, 1.0, r)) != PT_OK) return st;
-    cheb_first_kernel<double><<<vgrid(s->n), 256, 0, s->op->stream>>>(1.0, s->dinv, r, z, z, s->n);
+    if ((stt = sv_axpby<double>(s, -alpha, q, 1.0, r, n)) != PT_OK) return stt;
+    cheb_first_kernel<double><<<vgrid(n), 256, 0, st>>>(1.0, dinv, r, z, z, n);
     PT_LAUNCHED(s->op);
     double rz_new;
-    if ((st = sv_dot(s, r, z, &rz_new)) != PT_OK) return st;
+    if ((stt = sv_dot(s, r, z, &rz_new, n)) != PT_OK) return stt;
     const double beta = rz_new / rz;
-    if ((st = sv_axpby<double>(s, 1.0, z, beta, p)) != PT_OK) return st;
+    if ((stt = sv_axpby<double>(s, 1.0, z, beta, p, n)) != PT_OK) return stt;
     alphas.push_back(alpha);
     betas.push_back(beta);
     rz = rz_new;
@@ -334,7 +344,311 @@ pt_status sv_estimate_lambda(pt_solver *s)
     diag.push_back(t);
     if (k + 1 < m) off.push_back(std::sqrt(betas[k]) / alphas[k]);
   }
-  s->lambda_max = tridiag_lambda_max(diag, off);
+  *lmax = tridiag_lambda_max(diag, off);
+  return PT_OK;
+}
+
+pt_status sv_estimate_lambda(pt_solver *s) { return sv_lanczos(s, s->op, s->n, s->dinv, &s->lambda_max); }
+
+// ---- multigrid set-up -------------------------------------------------------
+
+void mg_free(pt_mg *mg)
+{
+  if (!mg) return;
+  if (mg->gexec) cudaGraphExecDestroy(mg->gexec);
+  for (pt_mg_level &L : mg->lv) {
+    void *p[] = {L.dinv64, L.dinv32, L.x, L.b, L.r, L.d, L.az, L.dl, L.t1, L.Ae, L.ye, L.Ainv};
+    for (void *q : p) cudaFree(q);
+    if (L.own && L.op) pt_op_destroy(L.op);
+  }
+  delete mg;
+}
+
+// Coarse level of level f: half the elements per axis, coordinates and
+// Dirichlet mask injected; vf_c (the coarse vertex viscosity) restricted from
+// vf_f and interpolated to the coarse Gauss points.
+pt_status mg_coarsen(const pt_op *f, const double *vf_f, double *vf_c, pt_op **out)
+{
+  pt_mesh_desc d{};
+  d.mx = f->mx / 2; d.my = f->my / 2; d.mz = f->mz / 2;
+  pt_op *c = nullptr;
+  pt_status st = pt_op_create(&d, &c);
+  if (st != PT_OK) return st;
+  *out = c;  // the caller owns it from here on
+  if ((st = pt_op_set_stream(c, (void *)f->stream)) != PT_OK) return st;
+  c->a11_kernel = f->a11_kernel;
+  const MgBox fb = mgbox(f), cb = mgbox(c);
+  inject_coords_kernel<<<vgrid(c->nnodes), 256, 0, c->stream>>>(fb, cb, f->d_coords, c->d_coords);
+  PT_LAUNCHED(c);
+  if ((st = finish_coords(c)) != PT_OK) return st;
+  restrict_vertex_kernel<<<vgrid((int64_t)(cb.mx + 1) * (cb.my + 1) * (cb.mz + 1)), 256, 0, c->stream>>>(fb, cb, vf_f,
+                                                                                                        vf_c);
+  PT_LAUNCHED(c);
+  eta_from_vertex_kernel<<<vgrid(27 * c->nel), 256, 0, c->stream>>>(cb, vf_c, c->d_eta);
+  PT_LAUNCHED(c);
+  if ((st = finish_eta(c)) != PT_OK) return st;
+  inject_mask_kernel<<<vgrid(c->nnodes), 256, 0, c->stream>>>(fb, cb, f->d_mask, c->d_mask);
+  PT_LAUNCHED(c);
+  c->has_mask = f->has_mask;
+  return PT_OK;
+}
+
+constexpr int64_t MG_EBE_MAX_ELEMENTS = 32768;  // levels up to 32^3 elements store element matrices
+constexpr int64_t MG_DENSE_MAX_DOFS = 1200;     // coarsest level solved by a dense inverse up to this size
+
+// Dense inverse of the coarsest level's masked operator (Dirichlet rows and
+// columns replaced by the identity), from its FP64 element matrices:
+// assembled on the host, Cholesky-factored, inverted, uploaded as T.
+pt_status mg_dense_inverse(pt_mg_level &L, bool fp32)
+{
+  const pt_op *op = L.op;
+  const int64_t n = L.n, nel = op->nel;
+  double *dAe = nullptr;
+  PT_CUDA(cudaMalloc(&dAe, sizeof(double) * 6561 * nel));
+  element_matrix_kernel<double><<<(unsigned)nel, 96, 0, op->stream>>>(op->box, op->d_coords, op->d_eta, dAe);
+  std::vector<double> Ae(6561 * nel), A(n * n, 0.0);
+  std::vector<uint8_t> mask(n);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaMemcpyAsync(Ae.data(), dAe, sizeof(double) * Ae.size(), cudaMemcpyDeviceToHost, op->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(mask.data(), op->d_mask, n, cudaMemcpyDeviceToHost, op->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(op->stream);
+  cudaFree(dAe);
+  if (e != cudaSuccess) return fail(PT_ERR_CUDA, "coarse element matrices: %s", cudaGetErrorString(e));
+  const int64_t X = op->box.X, XY = op->box.XY;
+  for (int64_t el = 0; el < nel; el++) {
+    const int64_t ei = el % op->mx, ej = (el / op->mx) % op->my, ek = el / ((int64_t)op->mx * op->my);
+    int64_t g[81];
+    for (int nn = 0; nn < 27; nn++) {
+      const int64_t node = (2 * ei + nn % 3) + (2 * ej + (nn / 3) % 3) * X + (2 * ek + nn / 9) * XY;
+      for (int l = 0; l < 3; l++) g[3 * nn + l] = 3 * node + l;
+    }
+    const double *m = &Ae[el * 6561];
+    for (int jj = 0; jj < 81; jj++) {
+      if (mask[g[jj]]) continue;
+      for (int ii = 0; ii < 81; ii++)
+        if (!mask[g[ii]]) A[g[ii] * n + g[jj]] += m[jj * 81 + ii];
+    }
+  }
+  for (int64_t i = 0; i < n; i++)
+    if (mask[i]) A[i * n + i] = 1.0;
+  // A = L L^T (lower triangle in place), W = L^-1, A^-1 = W^T W
+  for (int64_t j = 0; j < n; j++) {
+    double d = A[j * n + j];
+    for (int64_t k = 0; k < j; k++) d -= A[j * n + k] * A[j * n + k];
+    if (!(d > 0.0)) return fail(PT_ERR_STATE, "coarse operator is not positive definite");
+    d = std::sqrt(d);
+    A[j * n + j] = d;
+    for (int64_t i = j + 1; i < n; i++) {
+      double v = A[i * n + j];
+      for (int64_t k = 0; k < j; k++) v -= A[i * n + k] * A[j * n + k];
+      A[i * n + j] = v / d;
+    }
+  }
+  std::vector<double> W(n * n, 0.0);
+  for (int64_t c = 0; c < n; c++) {  // column c of L^-1 by forward substitution
+    W[c * n + c] = 1.0 / A[c * n + c];
+    for (int64_t i = c + 1; i < n; i++) {
+      double v = 0.0;
+      for (int64_t k = c; k < i; k++) v -= A[i * n + k] * W[k * n + c];
+      W[i * n + c] = v / A[i * n + i];
+    }
+  }
+  std::vector<double> inv(n * n, 0.0);
+  for (int64_t i = 0; i < n; i++)
+    for (int64_t j = 0; j <= i; j++) {
+      double v = 0.0;
+      for (int64_t k = i; k < n; k++) v += W[k * n + i] * W[k * n + j];
+      inv[i * n + j] = inv[j * n + i] = v;
+    }
+  const size_t ts = fp32 ? sizeof(float) : sizeof(double);
+  PT_CUDA(cudaMalloc(&L.Ainv, ts * n * n));
+  if (fp32) {
+    std::vector<float> f(inv.begin(), inv.end());
+    PT_CUDA(cudaMemcpy(L.Ainv, f.data(), ts * n * n, cudaMemcpyHostToDevice));
+  } else {
+    PT_CUDA(cudaMemcpy(L.Ainv, inv.data(), ts * n * n, cudaMemcpyHostToDevice));
+  }
+  return PT_OK;
+}
+
+// Work vectors, inverse diagonal and lambda_max(D^-1 A) of level L; element
+// matrices when the level is small; the dense inverse on a small coarsest level.
+pt_status mg_level_setup(pt_solver *s, pt_mg &mg, pt_mg_level &L, const pt_op *next)
+{
+  const size_t ts = mg.fp32 ? sizeof(float) : sizeof(double);
+  L.n = L.op->nvel;
+  L.nel = L.op->nel;
+  PT_CUDA(cudaMalloc(&L.dinv64, sizeof(double) * L.n));
+  PT_CUDA(cudaMalloc(&L.dinv32, sizeof(float) * L.n));
+  void **vecs[] = {&L.x, &L.b, &L.r, &L.d, &L.az, &L.dl};
+  for (void **v : vecs) PT_CUDA(cudaMalloc(v, ts * L.n));
+  if (next) {  // transfer temporaries: 3 (2mcx+1)(2my+1)(2mz+1) values each
+    const int64_t nt = 3LL * (2 * next->mx + 1) * (2 * L.op->my + 1) * (2 * L.op->mz + 1);
+    PT_CUDA(cudaMalloc(&L.t1, 2 * ts * nt));
+    L.t2 = (char *)L.t1 + ts * nt;
+  }
+  pt_status st = pt_getdiag_a11_d(L.op, s->t1);
+  if (st != PT_OK) return st;
+  reciprocal_kernel<<<vgrid(L.n), 256, 0, s->op->stream>>>(s->t1, L.dinv64, L.dinv32, L.n);
+  PT_LAUNCHED(s->op);
+  if ((st = sv_lanczos(s, L.op, L.n, L.dinv64, &L.lmax)) != PT_OK) return st;
+  if (!mg.assembled) return PT_OK;
+  if (!next && L.n <= MG_DENSE_MAX_DOFS && (st = mg_dense_inverse(L, mg.fp32)) != PT_OK) return st;
+  if (L.nel <= MG_EBE_MAX_ELEMENTS && !L.Ainv) {
+    PT_CUDA(cudaMalloc(&L.Ae, ts * 6561 * L.nel));
+    PT_CUDA(cudaMalloc(&L.ye, ts * 81 * L.nel));
+    if (mg.fp32)
+      element_matrix_kernel<float><<<(unsigned)L.nel, 96, 0, L.op->stream>>>(L.op->box, L.op->d_coords, L.op->d_eta,
+                                                                             (float *)L.Ae);
+    else
+      element_matrix_kernel<double><<<(unsigned)L.nel, 96, 0, L.op->stream>>>(L.op->box, L.op->d_coords,
+                                                                              L.op->d_eta, (double *)L.Ae);
+    PT_LAUNCHED(L.op);
+  }
+  return PT_OK;
+}
+
+pt_status mg_build(pt_solver *s)
+{
+  if (!s->op->full_box) return fail(PT_ERR_UNSUPPORTED, "multigrid needs a one-rank box (node box = element box)");
+  pt_mg *mg = new (std::nothrow) pt_mg();
+  if (!mg) return fail(PT_ERR_OOM, "host allocation failed");
+  s->mg = mg;  // freed by pt_solver_destroy, also after a failure here
+  mg->fp32 = s->o.cheby_fp32 != 0;
+  mg->degree = s->o.cheby_degree;
+  mg->coarse_degree = s->o.mg_coarse_degree > 0 ? s->o.mg_coarse_degree : 24;
+  mg->emin = s->o.cheby_emin;
+  mg->emax = s->o.cheby_emax;
+  mg->use_graph = s->o.pc_graph != 0;
+  mg->assembled = s->o.mg_assembled != 0;
+  const int maxl = s->o.mg_levels > 0 ? s->o.mg_levels : 32;
+  pt_mg_level L0{};
+  L0.op = s->op;
+  mg->lv.push_back(L0);
+  pt_status st = upload_q1_table();
+  if (st != PT_OK) return st;
+  // two vertex-field buffers (fine level's size), swapped level by level
+  const pt_op *op = s->op;
+  const int64_t nv0 = (int64_t)(op->mx + 1) * (op->my + 1) * (op->mz + 1);
+  double *vf[2] = {nullptr, nullptr};
+  PT_CUDA(cudaMalloc(&vf[0], sizeof(double) * 2 * nv0));
+  vf[1] = vf[0] + nv0;
+  vertex_field_kernel<<<vgrid(nv0), 256, 0, op->stream>>>(mgbox(op), op->d_eta, vf[0]);
+  st = cudaGetLastError() == cudaSuccess ? PT_OK : fail(PT_ERR_CUDA, "vertex field kernel launch failed");
+  while (st == PT_OK && (int)mg->lv.size() < maxl) {
+    const pt_op *f = mg->lv.back().op;
+    if ((f->mx & 1) || (f->my & 1) || (f->mz & 1) || f->mx < 4 || f->my < 4 || f->mz < 4) break;
+    pt_mg_level L{};
+    L.own = true;
+    mg->lv.push_back(L);
+    const int cur = ((int)mg->lv.size() - 2) & 1;
+    st = mg_coarsen(f, vf[cur], vf[cur ^ 1], &mg->lv.back().op);
+  }
+  if (st == PT_OK && cudaStreamSynchronize(op->stream) != cudaSuccess) st = fail(PT_ERR_CUDA, "multigrid set-up failed");
+  cudaFree(vf[0]);
+  if (st != PT_OK) return st;
+  for (size_t l = 0; l < mg->lv.size(); l++) {
+    const pt_op *next = l + 1 < mg->lv.size() ? mg->lv[l + 1].op : nullptr;
+    if ((st = mg_level_setup(s, *mg, mg->lv[l], next)) != PT_OK) return st;
+  }
+  s->lambda_max = mg->lv[0].lmax;
+  return PT_OK;
+}
+
+// Capture one V-cycle (level-0 b -> level-0 x) as a CUDA graph.  A first
+// eager cycle sets every kernel attribute; the capture runs on a private
+// stream (the levels' stream is swapped for the capture and put back).
+template <typename T>
+pt_status mg_capture(pt_solver *s)
+{
+  pt_mg &mg = *s->mg;
+  pt_status st = mg_vcycle<T>(mg, 0);
+  if (st != PT_OK) return st;
+  PT_CUDA(cudaStreamSynchronize(s->op->stream));
+  cudaStream_t cap;
+  PT_CUDA(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
+  std::vector<cudaStream_t> saved;
+  for (pt_mg_level &L : mg.lv) {
+    saved.push_back(L.op->stream);
+    L.op->stream = cap;
+  }
+  const int64_t f0 = mg.fine_applies;
+  const double c0 = mg.coarse_work;
+  cudaGraph_t g = nullptr;
+  cudaError_t e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal);
+  if (e == cudaSuccess) {
+    st = mg_vcycle<T>(mg, 0);
+    e = cudaStreamEndCapture(cap, &g);
+  }
+  for (size_t i = 0; i < mg.lv.size(); i++) mg.lv[i].op->stream = saved[i];
+  mg.graph_fine = mg.fine_applies - f0;
+  mg.graph_coarse = mg.coarse_work - c0;
+  mg.fine_applies = f0;
+  mg.coarse_work = c0;
+  if (e == cudaSuccess && st == PT_OK) e = cudaGraphInstantiate(&mg.gexec, g, 0);
+  if (g) cudaGraphDestroy(g);
+  cudaStreamDestroy(cap);
+  if (st != PT_OK) return st;
+  if (e != cudaSuccess) return fail(PT_ERR_CUDA, "V-cycle graph capture: %s", cudaGetErrorString(e));
+  return PT_OK;
+}
+
+template <typename T>
+pt_status mg_run(pt_solver *s)
+{
+  pt_mg &mg = *s->mg;
+  if (!mg.use_graph) return mg_vcycle<T>(mg, 0);
+  if (!mg.gexec) {
+    pt_status st = mg_capture<T>(s);
+    if (st != PT_OK) return st;
+  }
+  PT_CUDA(cudaGraphLaunch(mg.gexec, s->op->stream));
+  mg.fine_applies += mg.graph_fine;
+  mg.coarse_work += mg.graph_coarse;
+  return PT_OK;
+}
+
+// Preconditioner set-up (PCSetUp): inverse diagonal, lambda_max or the level
+// hierarchy; redone when the op's coordinates, viscosity or mask changed.
+pt_status sv_setup(pt_solver *s)
+{
+  if (s->setup_done && s->op_state == s->op->state) return PT_OK;
+  s->have_diag = false;
+  s->lambda_max = 0.0;
+  mg_free(s->mg);
+  s->mg = nullptr;
+  s->setup_done = false;
+  pt_status st = PT_OK;
+  if (s->o.pc != PT_PC_NONE && (st = sv_setup_diag(s)) != PT_OK) return st;
+  if (s->o.pc == PT_PC_CHEBY_JACOBI && (st = sv_estimate_lambda(s)) != PT_OK) return st;
+  if (s->o.pc == PT_PC_MG && (st = mg_build(s)) != PT_OK) {
+    mg_free(s->mg);
+    s->mg = nullptr;
+    return st;
+  }
+  s->setup_done = true;
+  s->op_state = s->op->state;
+  return PT_OK;
+}
+
+pt_status sv_precond_mg(pt_solver *s, const double *r, double *z)
+{
+  pt_mg &mg = *s->mg;
+  pt_mg_level &L0 = mg.lv[0];
+  cudaStream_t st = s->op->stream;
+  if (mg.fp32) {
+    convert_kernel<float, double><<<vgrid(s->n), 256, 0, st>>>(r, (float *)L0.b, s->n);
+    PT_LAUNCHED(s->op);
+    pt_status stt = mg_run<float>(s);
+    if (stt != PT_OK) return stt;
+    convert_kernel<double, float><<<vgrid(s->n), 256, 0, st>>>((float *)L0.x, z, s->n);
+    PT_LAUNCHED(s->op);
+  } else {
+    PT_CUDA(cudaMemcpyAsync(L0.b, r, sizeof(double) * s->n, cudaMemcpyDeviceToDevice, st));
+    pt_status stt = mg_run<double>(s);
+    if (stt != PT_OK) return stt;
+    PT_CUDA(cudaMemcpyAsync(z, L0.x, sizeof(double) * s->n, cudaMemcpyDeviceToDevice, st));
+  }
   return PT_OK;
 }
 
@@ -346,6 +660,7 @@ pt_status sv_precond(pt_solver *s, const double *r, double *z)
     PT_CUDA(cudaMemcpyAsync(z, r, sizeof(double) * s->n, cudaMemcpyDeviceToDevice, s->op->stream));
     return PT_OK;
   }
+  if (o.pc == PT_PC_MG) return sv_precond_mg(s, r, z);
   if (o.pc == PT_PC_JACOBI) {
     cheb_first_kernel<double><<<vgrid(s->n), 256, 0, s->op->stream>>>(1.0, s->dinv, r, z, z, s->n);
     PT_LAUNCHED(s->op);
@@ -540,6 +855,10 @@ void pt_solve_opts_default(pt_solve_opts *o)
   o->cheby_emin = 0.2;
   o->cheby_emax = 1.1;
   o->eig_its = 20;
+  o->mg_levels = 0;
+  o->mg_coarse_degree = 24;
+  o->pc_graph = 1;
+  o->mg_assembled = 1;
 }
 
 pt_status pt_solver_create(pt_op *op, const pt_solve_opts *opts, pt_solver **out)
@@ -547,7 +866,7 @@ pt_status pt_solver_create(pt_op *op, const pt_solve_opts *opts, pt_solver **out
   if (!op || !opts || !out) return fail(PT_ERR_BAD_ARG, "NULL argument");
   *out = nullptr;
   if (opts->ksp != PT_KSP_FGMRES && opts->ksp != PT_KSP_FCG) return fail(PT_ERR_BAD_ARG, "unknown ksp %d", opts->ksp);
-  if (opts->pc < PT_PC_NONE || opts->pc > PT_PC_CHEBY_JACOBI) return fail(PT_ERR_BAD_ARG, "unknown pc %d", opts->pc);
+  if (opts->pc < PT_PC_NONE || opts->pc > PT_PC_MG) return fail(PT_ERR_BAD_ARG, "unknown pc %d", opts->pc);
   if (opts->restart < 1 || opts->restart > 256) return fail(PT_ERR_BAD_ARG, "restart must be in [1, 256]");
   if (opts->cheby_degree < 1 || opts->cheby_degree > 64) return fail(PT_ERR_BAD_ARG, "cheby_degree must be in [1, 64]");
   if (!(opts->cheby_emin > 0.0) || !(opts->cheby_emax > opts->cheby_emin))
@@ -585,6 +904,15 @@ pt_status pt_solver_create(pt_op *op, const pt_solve_opts *opts, pt_solver **out
   return PT_OK;
 }
 
+pt_status pt_solver_apply_pc_d(pt_solver *s, const double *r, double *z)
+{
+  if (!s || !r || !z) return fail(PT_ERR_BAD_ARG, "NULL argument");
+  if (r == z) return fail(PT_ERR_BAD_ARG, "r and z must not alias");
+  pt_status st = sv_setup(s);
+  if (st != PT_OK) return st;
+  return sv_precond(s, r, z);
+}
+
 pt_status pt_solver_destroy(pt_solver *s)
 {
   if (!s) return PT_OK;
@@ -593,6 +921,7 @@ pt_status pt_solver_destroy(pt_solver *s)
                   s->az32, s->partial, s->dres, s->hbuf, (void *)s->dptr};
   for (void *p : ptrs) cudaFree(p);
   if (s->hhost) cudaFreeHost(s->hhost);
+  mg_free(s->mg);
   delete s;
   return PT_OK;
 }
@@ -603,13 +932,12 @@ pt_status pt_solver_solve_d(pt_solver *s, const double *b, double *x, pt_solve_s
   memset(stats, 0, sizeof *stats);
   const auto t0 = std::chrono::steady_clock::now();
   s->n64 = s->n32 = 0;
-  pt_status st;
-  if (s->o.pc != PT_PC_NONE) {
-    if ((st = sv_setup_diag(s)) != PT_OK) return st;
+  if (s->mg) {
+    s->mg->fine_applies = 0;
+    s->mg->coarse_work = 0.0;
   }
-  if (s->o.pc == PT_PC_CHEBY_JACOBI && !(s->lambda_max > 0.0)) {
-    if ((st = sv_estimate_lambda(s)) != PT_OK) return st;
-  }
+  pt_status st = sv_setup(s);
+  if (st != PT_OK) return st;
   stats->lambda_max = s->lambda_max;
   if (s->o.ksp == PT_KSP_FGMRES) st = sv_fgmres(s, b, x, stats);
   else st = sv_fcg(s, b, x, stats);
@@ -617,6 +945,11 @@ pt_status pt_solver_solve_d(pt_solver *s, const double *b, double *x, pt_solve_s
   PT_CUDA(cudaStreamSynchronize(s->op->stream));
   stats->a11_f64 = s->n64;
   stats->a11_f32 = s->n32;
+  if (s->mg) {
+    (s->mg->fp32 ? stats->a11_f32 : stats->a11_f64) += s->mg->fine_applies;
+    stats->a11_coarse = s->mg->coarse_work;
+    stats->mg_levels = (int32_t)s->mg->lv.size();
+  }
   stats->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
   return PT_OK;
 }

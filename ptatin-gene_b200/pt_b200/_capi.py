@@ -30,13 +30,16 @@ class SolveOpts(ctypes.Structure):
     _fields_ = [("ksp", ctypes.c_int32), ("restart", ctypes.c_int32), ("max_it", ctypes.c_int32),
                 ("rtol", ctypes.c_double), ("atol", ctypes.c_double), ("pc", ctypes.c_int32),
                 ("cheby_degree", ctypes.c_int32), ("cheby_fp32", ctypes.c_int32),
-                ("cheby_emin", ctypes.c_double), ("cheby_emax", ctypes.c_double), ("eig_its", ctypes.c_int32)]
+                ("cheby_emin", ctypes.c_double), ("cheby_emax", ctypes.c_double), ("eig_its", ctypes.c_int32),
+                ("mg_levels", ctypes.c_int32), ("mg_coarse_degree", ctypes.c_int32), ("pc_graph", ctypes.c_int32),
+                ("mg_assembled", ctypes.c_int32)]
 
 
 class SolveStats(ctypes.Structure):
     _fields_ = [("its", ctypes.c_int32), ("converged", ctypes.c_int32), ("rnorm0", ctypes.c_double),
                 ("rnorm", ctypes.c_double), ("lambda_max", ctypes.c_double), ("a11_f64", ctypes.c_int64),
-                ("a11_f32", ctypes.c_int64), ("seconds", ctypes.c_double)]
+                ("a11_f32", ctypes.c_int64), ("seconds", ctypes.c_double), ("mg_levels", ctypes.c_int32),
+                ("reserved", ctypes.c_int32), ("a11_coarse", ctypes.c_double)]
 
 
 _vp = ctypes.c_void_p
@@ -76,6 +79,7 @@ SIGNATURES = {
     "pt_solve_opts_default": [ctypes.POINTER(SolveOpts)],
     "pt_solver_create": [_vp, ctypes.POINTER(SolveOpts), ctypes.POINTER(_vp)],
     "pt_solver_solve_d": [_vp, _vp, _vp, ctypes.POINTER(SolveStats)],
+    "pt_solver_apply_pc_d": [_vp, _vp, _vp],
     "pt_solver_destroy": [_vp],
     "pt_batch_create": [ctypes.c_int, _vp, _vp, ctypes.POINTER(_vp)],
     "pt_batch_destroy": [_vp],

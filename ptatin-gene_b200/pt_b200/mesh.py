@@ -249,8 +249,9 @@ def problem(config: str, seed: int = 0):
     Returns (mesh, eta, mask).  Names: ``c0`` 8^3 perturbed +-0.1h with
     log-uniform eta in [1e-2, 1e2]; ``c1`` 64^3 undeformed sinker (16 spheres,
     r 0.08, eta 1e4); ``c2`` 128^3 perturbed +-0.05h layered with 64
-    inclusions (contrast 1e6); ``cN:mx,my,mz`` a small perturbed box with
-    log-uniform eta.
+    inclusions (contrast 1e6); ``box:mx,my,mz`` a perturbed box with
+    log-uniform eta; ``sinker:mx,my,mz`` and ``layered:mx,my,mz`` the c1 and
+    c2 viscosity fields on a box of that size (perturbed +-0.05h).
     """
     if config == "c0":
         m = make_mesh(8, 8, 8, perturb=0.1, seed=seed)
@@ -265,6 +266,11 @@ def problem(config: str, seed: int = 0):
         mx, my, mz = (int(v) for v in config[4:].split(","))
         m = make_mesh(mx, my, mz, perturb=0.1, seed=seed)
         eta = eta_loguniform_qp(m, -2.0, 2.0, seed=seed + 1)
+    elif config.startswith(("sinker:", "layered:")):
+        kind, dims = config.split(":")
+        mx, my, mz = (int(v) for v in dims.split(","))
+        m = make_mesh(mx, my, mz, perturb=0.05, seed=seed)
+        eta = (eta_sinker if kind == "sinker" else eta_layered)(m, seed=seed + 1)
     else:
         raise ValueError(f"unknown workload {config!r}")
     return m, eta, bc_mask_freeslip(*m.dims)

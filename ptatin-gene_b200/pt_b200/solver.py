@@ -3,8 +3,10 @@
 ``KSPSolveA11`` mirrors how the reference drives the A11 shell inside its
 viscous-block solve (FGMRES outer, Chebyshev-Jacobi smoothing with the
 eigenvalue window 0.2..1.1 of the estimated lambda_max; see
-src/ptatin_driver_linear_ts.c:559-883), on the fine level only, with the
-smoother optionally in FP32.
+src/ptatin_driver_linear_ts.c:559-883), with the smoother optionally in FP32.
+``pc="cheby_jacobi"`` smooths the fine level only; ``pc="mg"`` is the
+reference's geometric V-cycle over re-discretised Q2 levels (coordinates
+injected, Gauss-point viscosity projected, the same kernels on each level).
 """
 from __future__ import annotations
 
@@ -14,7 +16,7 @@ from . import _capi
 from .operator import _dptr
 
 KSP = {"fgmres": 0, "fcg": 1}
-PC = {"none": 0, "jacobi": 1, "cheby_jacobi": 2}
+PC = {"none": 0, "jacobi": 1, "cheby_jacobi": 2, "mg": 3}
 
 
 def default_opts(**kw):
@@ -46,6 +48,12 @@ class KSPSolveA11:
         st = _capi.SolveStats()
         _capi.call("pt_solver_solve_d", self._h, _dptr(b, torch.float64), _dptr(x, torch.float64), ctypes.byref(st))
         return {f: getattr(st, f) for f, _ in _capi.SolveStats._fields_}
+
+    def apply_pc(self, r, z):
+        """z = P r (PCApply) with the configured preconditioner; float64 CUDA
+        tensors on the op's device."""
+        import torch
+        _capi.call("pt_solver_apply_pc_d", self._h, _dptr(r, torch.float64), _dptr(z, torch.float64))
 
     def destroy(self):
         if getattr(self, "_h", None):

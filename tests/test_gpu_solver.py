@@ -97,3 +97,151 @@ def test_solve_is_bitwise_repeatable():
         torch.cuda.synchronize()
         assert s1["its"] == s2["its"]
         assert torch.equal(x1, x2)
+
+
+@pytest.mark.parametrize("ksp", ["fgmres", "fcg"])
+@pytest.mark.parametrize("fp32", [0, 1])
+def test_mg_solve_reaches_rtol(ora, ksp, fp32):
+    """Geometric V-cycle (re-discretised Q2 levels 16 -> 8 -> 4 -> 2) as the
+    preconditioner: converges to rtol 1e-8 on the true FP64 residual."""
+    import torch
+
+    from pt_b200.solver import KSPSolveA11
+    m, eta, mask, f, op, fd = setup("box:16,16,16", seed=7)
+    x = torch.zeros_like(fd)
+    with op, KSPSolveA11(op, ksp=ksp, pc="mg", cheby_fp32=fp32, rtol=1e-8, max_it=500) as k:
+        st = k.solve(fd, x)
+        assert st["converged"] == 1, st
+        assert st["mg_levels"] == 4
+        assert st["a11_coarse"] > 0
+        assert true_relres(ora, m, eta, mask, f, x.cpu().numpy()) < 2e-8
+        assert (st["a11_f32"] > 0) == bool(fp32)
+
+
+def test_mg_needs_far_fewer_iterations_than_single_level():
+    """A correct coarse-grid correction (prolongation, restriction, coarse
+    operators) cuts the outer iteration count several-fold against the
+    single-level Chebyshev-Jacobi preconditioner of the same degree."""
+    import torch
+
+    from pt_b200.solver import KSPSolveA11
+    m, eta, mask, f, op, fd = setup("box:16,16,16", seed=8)
+    with op:
+        x1 = torch.zeros_like(fd)
+        x2 = torch.zeros_like(fd)
+        with KSPSolveA11(op, pc="cheby_jacobi", max_it=5000) as k:
+            s1 = k.solve(fd, x1)
+        with KSPSolveA11(op, pc="mg", max_it=5000) as k:
+            s2 = k.solve(fd, x2)
+        assert s1["converged"] and s2["converged"], (s1, s2)
+        assert s2["its"] * 4 <= s1["its"], (s1["its"], s2["its"])
+        assert relerr(x2.cpu().numpy(), x1.cpu().numpy()) < 1e-5
+
+
+def test_mg_is_bitwise_repeatable_and_handles_odd_meshes(ora):
+    import torch
+
+    from pt_b200.solver import KSPSolveA11
+    m, eta, mask, f, op, fd = setup("box:12,9,8", seed=9)   # 9 is odd: one level
+    with op, KSPSolveA11(op, pc="mg", ksp="fcg", max_it=3000) as k:
+        x1 = torch.zeros_like(fd)
+        x2 = torch.zeros_like(fd)
+        s1 = k.solve(fd, x1)
+        s2 = k.solve(fd, x2)
+        torch.cuda.synchronize()
+        assert s1["converged"] and s1["mg_levels"] == 1
+        assert s1["its"] == s2["its"] and torch.equal(x1, x2)
+        assert true_relres(ora, m, eta, mask, f, x1.cpu().numpy()) < 2e-8
+
+
+def test_mg_vcycle_is_symmetric_and_graph_replay_is_bitwise():
+    """With FP64 smoothing the V-cycle is a symmetric operator (restriction is
+    the transpose of prolongation, pre- and post-smoother are the same
+    polynomial), and the captured-graph replay gives bitwise the eager result."""
+    import torch
+
+    from pt_b200.solver import KSPSolveA11
+    m, eta, mask, f, op, fd = setup("layered:16,16,8", seed=10)
+    free = torch.from_numpy((mask == 0).astype(np.float64)).cuda()
+    g = torch.Generator(device="cpu").manual_seed(3)
+    r1 = (torch.rand(m.nvel, generator=g, dtype=torch.float64) - 0.5).cuda() * free
+    r2 = (torch.rand(m.nvel, generator=g, dtype=torch.float64) - 0.5).cuda() * free
+    with op:
+        z = {}
+        for graph in (0, 1):
+            with KSPSolveA11(op, pc="mg", cheby_fp32=0, pc_graph=graph) as k:
+                z1 = torch.empty_like(r1)
+                z2 = torch.empty_like(r2)
+                k.apply_pc(r1, z1)
+                k.apply_pc(r2, z2)
+                k.apply_pc(r1, z1)   # second replay of the same input
+                torch.cuda.synchronize()
+                z[graph] = (z1, z2)
+        assert torch.equal(z[0][0], z[1][0]) and torch.equal(z[0][1], z[1][1])
+        a = torch.dot(z[1][0], r2).item()
+        b = torch.dot(r1, z[1][1]).item()
+        assert abs(a - b) <= 1e-10 * max(abs(a), abs(b)), (a, b)
+        assert torch.dot(z[1][0], r1).item() > 0.0
+
+
+def test_pc_setup_follows_viscosity_changes(ora):
+    """A solver set up for one viscosity re-does its set-up (diagonal,
+    eigenvalue estimates, level hierarchy) after the op's viscosity changes,
+    and then gives bitwise the result of a fresh solver."""
+    import torch
+
+    from pt_b200.solver import KSPSolveA11
+    m, eta, mask, f, op, fd = setup("layered:8,8,8", seed=11)
+    eta2 = eta * np.exp(np.sin(np.arange(eta.size) * 0.37))
+    with op:
+        with KSPSolveA11(op, pc="mg") as k:
+            x = torch.zeros_like(fd)
+            k.solve(fd, x)
+            op.set_eta(eta2)
+            x1 = torch.zeros_like(fd)
+            s1 = k.solve(fd, x1)
+        with KSPSolveA11(op, pc="mg") as k2:
+            x2 = torch.zeros_like(fd)
+            s2 = k2.solve(fd, x2)
+        torch.cuda.synchronize()
+        assert s1["converged"] and s1["its"] == s2["its"] and torch.equal(x1, x2)
+        assert true_relres(ora, m, eta2, mask, f, x1.cpu().numpy()) < 2e-8
+
+
+def test_mg_assembled_levels_match_matrix_free_levels():
+    """Element-matrix levels apply the same operator as the matrix-free
+    kernels: with FP64 smoothing the V-cycles agree to rounding."""
+    import torch
+
+    from pt_b200.solver import KSPSolveA11
+    m, eta, mask, f, op, fd = setup("layered:8,8,8", seed=12)
+    with op:
+        z = {}
+        for asm in (0, 1):
+            with KSPSolveA11(op, pc="mg", cheby_fp32=0, mg_levels=2, mg_assembled=asm) as k:
+                out = torch.empty_like(fd)
+                k.apply_pc(fd, out)
+                torch.cuda.synchronize()
+                z[asm] = out.cpu().numpy()
+        assert relerr(z[1], z[0]) < 1e-11
+
+
+def test_mg_dense_coarsest_level_is_an_exact_solve(ora):
+    """One level of 2^3 elements (375 dofs) is solved by its dense inverse:
+    the preconditioned iteration converges at once to the direct solution."""
+    import torch
+
+    from pt_b200.solver import KSPSolveA11
+    m, eta, mask, f, op, fd = setup("box:2,2,2", seed=13)
+    n = m.nvel
+    A = np.zeros((n, n))
+    for j in range(n):
+        e = np.zeros(n)
+        e[j] = 1.0
+        A[:, j] = ora.matmult_a11(m.dims, m.coords, eta, mask, e)
+    xref = np.linalg.solve(A, f)
+    with op, KSPSolveA11(op, pc="mg", ksp="fcg", mg_levels=1, cheby_fp32=0, rtol=1e-10) as k:
+        x = torch.zeros_like(fd)
+        st = k.solve(fd, x)
+    assert st["converged"] and st["its"] <= 2, st
+    assert relerr(x.cpu().numpy(), xref) < 1e-10
