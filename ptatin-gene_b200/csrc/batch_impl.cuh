@@ -36,6 +36,8 @@ pt_status batch_launch_cls(const pt_batch *b, const pt_batch::Cls &c, const T *c
   if (dev < 64 && !attr_set[dev]) {
     PT_CUDA(cudaFuncSetAttribute(ptk::a11_stream_batch_kernel<T, TX, MASKED>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    PT_CUDA(cudaFuncSetAttribute(ptk::a11_stream_batch_kernel<T, TX, MASKED>,
+                                 cudaFuncAttributePreferredSharedMemoryCarveout, (int)cudaSharedmemCarveoutMaxShared));
     attr_set[dev] = true;
   }
   const ptk::BatchProb *probs = std::is_same<T, double>::value ? b->d_probs64 : b->d_probs32;

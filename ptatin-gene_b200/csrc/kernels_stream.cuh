@@ -338,8 +338,19 @@ __device__ __forceinline__ void stream_tile(const StreamGrid &g, int tx, int ej,
   }
 }
 
+// Resident CTAs per SM the register budget is sized for.  FP64 keeps one
+// quadrature plane's gradient (81 doubles) live: 256 threads per SM.  FP32
+// rows of 128 elements fit 4 CTAs (512 threads, 128 registers, 4 x 55.8 KB
+// of tiles) -- measured 1.34x faster than 2 CTAs at 128^3; narrower FP32
+// tiles measured best at 256 threads per SM.
+template <typename T, int TX>
+constexpr int stream_min_blocks()
+{
+  return (sizeof(T) == 4 && TX == 128) ? 4 : 256 / TX;
+}
+
 template <typename T, int TX, bool MASKED>
-__global__ void __launch_bounds__(TX, 256 / TX) a11_stream_kernel(StreamGrid g, const T *__restrict__ K,
+__global__ void __launch_bounds__(TX, stream_min_blocks<T, TX>()) a11_stream_kernel(StreamGrid g, const T *__restrict__ K,
                                                                   const T *__restrict__ u,
                                                                   const uint8_t *__restrict__ mask,
                                                                   T *__restrict__ y)
@@ -365,7 +376,7 @@ struct BatchProb {
 };
 
 template <typename T, int TX, bool MASKED>
-__global__ void __launch_bounds__(TX, 256 / TX) a11_stream_batch_kernel(const BatchProb *__restrict__ probs,
+__global__ void __launch_bounds__(TX, stream_min_blocks<T, TX>()) a11_stream_batch_kernel(const BatchProb *__restrict__ probs,
                                                                         const int4 *__restrict__ items, int px, int py,
                                                                         int pz, const T *const *__restrict__ uptr,
                                                                         T *const *__restrict__ yptr)

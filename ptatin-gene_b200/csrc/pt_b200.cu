@@ -162,6 +162,8 @@ pt_status launch_stream_tx(pt_op *op, const T *K, const T *u, T *y)
   if (op->device < 64 && !attr_set[op->device]) {
     PT_CUDA(cudaFuncSetAttribute(ptk::a11_stream_kernel<T, TX, MASKED>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)smem));
+    PT_CUDA(cudaFuncSetAttribute(ptk::a11_stream_kernel<T, TX, MASKED>,
+                                 cudaFuncAttributePreferredSharedMemoryCarveout, (int)cudaSharedmemCarveoutMaxShared));
     attr_set[op->device] = true;
   }
   ptk::StreamGrid g;
