@@ -250,6 +250,55 @@ int64_t pt_batch_tiles(const pt_batch *batch);
 pt_status pt_batch_a11_apply_d(pt_batch *batch, const double *const *u, double *const *y, int masked, void *stream);
 pt_status pt_batch_a11_apply_f32_d(pt_batch *batch, const float *const *u, float *const *y, int masked, void *stream);
 
+/* ---- serving: continuously batched viscous solves ------------------------
+ * No counterpart in the reference (one solve per process there).  A server
+ * takes requests (A11 u = f on a one-rank box, mask = Dirichlet dofs, f zero
+ * there) as they arrive, admits them in FIFO order while slots and the
+ * device-memory budget allow, keeps each request's mesh data and Krylov
+ * state on the device, and advances all admitted requests together: one
+ * flexible-CG iteration (FP64 residuals and dots, Chebyshev(cheby_degree)-
+ * Jacobi preconditioner in FP32 or FP64) is one batched A11 work-list plus a
+ * fixed number of chunk-list vector kernels for the whole batch.  Each
+ * request's result is bitwise the same alone and in any mix. */
+typedef struct {
+  int64_t memory_budget_bytes; /* device bytes for admitted requests (default 120 GiB) */
+  int32_t max_active;          /* requests iterated together (default 256) */
+  int32_t lz;                  /* element layers per z-chunk of the A11 tiles (0: per-box default) */
+  int32_t cheby_fp32, cheby_degree;
+  double cheby_emin, cheby_emax;
+  int32_t eig_its;
+  double rtol, atol;
+  int32_t max_it;
+} pt_server_opts;
+
+typedef struct {
+  int64_t id;                  /* -1: nothing finished */
+  int32_t its, status;         /* status 1 converged, 2 max_it, 3 breakdown */
+  int32_t converged, reserved;
+  double rnorm0, rnorm;        /* FP64 residual norms (recurrence), initial and final */
+  double lambda_max;
+  double t_submit, t_admit, t_done; /* seconds on the server clock (pt_server_time) */
+} pt_server_result;
+
+typedef struct pt_server pt_server;
+
+void pt_server_opts_default(pt_server_opts *opts);
+pt_status pt_server_create(const pt_server_opts *opts, pt_server **server);
+pt_status pt_server_destroy(pt_server *server);
+/* Seconds since the server was created. */
+double pt_server_time(const pt_server *server);
+/* Queue a request.  The host arrays (coords 3N, eta 27 nel, mask 3N or NULL,
+ * f 3N) must stay valid until the request is admitted; x (3N) receives the
+ * solution and must stay valid until pt_server_next_done returns its id. */
+pt_status pt_server_submit(pt_server *server, int64_t id, const pt_mesh_desc *desc, const double *coords,
+                           const double *eta, const uint8_t *mask, const double *f, double *x);
+/* Enqueue `iterations` iterations of the admitted requests, admit queued
+ * requests while they run, wait, and retire the finished ones. */
+pt_status pt_server_step(pt_server *server, int32_t iterations, int32_t *n_active, int32_t *n_queued);
+/* Next finished request (res->id = -1 when none). */
+pt_status pt_server_next_done(pt_server *server, pt_server_result *res);
+pt_status pt_server_stats(const pt_server *server, int64_t *iterations, int64_t *launches, int64_t *bytes_in_use);
+
 /* ---- selection, in the style of -a11_op --------------------------------- */
 
 /* Select the A11 kernel by name, like the reference's -a11_op function list

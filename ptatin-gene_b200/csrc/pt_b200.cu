@@ -7,6 +7,7 @@
 // streams and the BC fix-ups of the MatShell-level calls.
 #include <cuda_runtime.h>
 
+#include <cmath>
 #include <cstdarg>
 #include <cstdio>
 #include <cstdlib>
@@ -904,3 +905,4 @@ extern "C" pt_status pt_a11_apply_noalloc_d(const pt_mesh_desc *desc, const doub
 
 #include "solver_impl.cuh"
 #include "batch_impl.cuh"
+#include "server_impl.cuh"

@@ -42,8 +42,23 @@ class SolveStats(ctypes.Structure):
                 ("reserved", ctypes.c_int32), ("a11_coarse", ctypes.c_double)]
 
 
+class ServerOpts(ctypes.Structure):
+    _fields_ = [("memory_budget_bytes", ctypes.c_int64), ("max_active", ctypes.c_int32), ("lz", ctypes.c_int32),
+                ("cheby_fp32", ctypes.c_int32), ("cheby_degree", ctypes.c_int32),
+                ("cheby_emin", ctypes.c_double), ("cheby_emax", ctypes.c_double), ("eig_its", ctypes.c_int32),
+                ("rtol", ctypes.c_double), ("atol", ctypes.c_double), ("max_it", ctypes.c_int32)]
+
+
+class ServerResult(ctypes.Structure):
+    _fields_ = [("id", ctypes.c_int64), ("its", ctypes.c_int32), ("status", ctypes.c_int32),
+                ("converged", ctypes.c_int32), ("reserved", ctypes.c_int32), ("rnorm0", ctypes.c_double),
+                ("rnorm", ctypes.c_double), ("lambda_max", ctypes.c_double), ("t_submit", ctypes.c_double),
+                ("t_admit", ctypes.c_double), ("t_done", ctypes.c_double)]
+
+
 _vp = ctypes.c_void_p
 _i64p = ctypes.POINTER(ctypes.c_int64)
+_i32p = ctypes.POINTER(ctypes.c_int32)
 
 # name -> argtypes (all return int status unless listed in _RESTYPES)
 SIGNATURES = {
@@ -87,6 +102,14 @@ SIGNATURES = {
     "pt_batch_tiles": [_vp],
     "pt_batch_a11_apply_d": [_vp, _vp, _vp, ctypes.c_int, _vp],
     "pt_batch_a11_apply_f32_d": [_vp, _vp, _vp, ctypes.c_int, _vp],
+    "pt_server_opts_default": [ctypes.POINTER(ServerOpts)],
+    "pt_server_create": [ctypes.POINTER(ServerOpts), ctypes.POINTER(_vp)],
+    "pt_server_destroy": [_vp],
+    "pt_server_time": [_vp],
+    "pt_server_submit": [_vp, ctypes.c_int64, ctypes.POINTER(MeshDesc), _vp, _vp, _vp, _vp, _vp],
+    "pt_server_step": [_vp, ctypes.c_int32, _i32p, _i32p],
+    "pt_server_next_done": [_vp, ctypes.POINTER(ServerResult)],
+    "pt_server_stats": [_vp, _i64p, _i64p, _i64p],
     "pt_op_set_a11_kernel": [_vp, ctypes.c_char_p],
     "pt_op_get_a11_kernel": [_vp],
     "pt_op_launch_count": [_vp],
@@ -103,6 +126,8 @@ _RESTYPES = {
     "pt_solve_opts_default": None,
     "pt_batch_launches_per_apply": ctypes.c_int64,
     "pt_batch_tiles": ctypes.c_int64,
+    "pt_server_opts_default": None,
+    "pt_server_time": ctypes.c_double,
 }
 
 _lib = None

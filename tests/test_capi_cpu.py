@@ -37,3 +37,44 @@ def test_bad_args_rejected_without_device():
     assert st == 1 and b"element counts" in lib.pt_last_error()
     assert lib.pt_op_create(None, ctypes.byref(h)) == 1
     assert lib.pt_a11_apply_d(None, None, None) == 1
+
+
+def test_struct_layouts_match_the_header(tmp_path):
+    """The ctypes mirrors have the C structs' sizes and field offsets
+    (checked against gcc on include/pt_b200.h)."""
+    import subprocess
+
+    from pt_b200 import _capi
+    structs = {"pt_mesh_desc": _capi.MeshDesc, "pt_solve_opts": _capi.SolveOpts,
+               "pt_solve_stats": _capi.SolveStats, "pt_server_opts": _capi.ServerOpts,
+               "pt_server_result": _capi.ServerResult}
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "pt_b200.h"', "int main(void) {"]
+    for cname, cls in structs.items():
+        lines.append(f'printf("{cname} size %zu\\n", sizeof({cname}));')
+        for f, _ in cls._fields_:
+            if f == "reserved":
+                continue
+            lines.append(f'printf("{cname} {f} %zu\\n", offsetof({cname}, {f}));')
+    lines.append("return 0; }")
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-I", os.path.join(REPO, "include"), str(src), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split("\n")
+    for line in filter(None, out):
+        cname, field, val = line.split()
+        cls = structs[cname]
+        got = ctypes.sizeof(cls) if field == "size" else getattr(cls, field).offset
+        assert got == int(val), (cname, field, got, val)
+
+
+def test_server_option_validation_without_device():
+    from pt_b200 import _capi
+    lib = _capi.load()
+    o = _capi.ServerOpts()
+    lib.pt_server_opts_default(ctypes.byref(o))
+    assert o.max_active == 256 and o.memory_budget_bytes == 120 << 30 and o.rtol == 1e-8
+    o.max_active = 0
+    h = ctypes.c_void_p()
+    assert lib.pt_server_create(ctypes.byref(o), ctypes.byref(h)) == 1
+    assert b"max_active" in lib.pt_last_error()
