@@ -434,6 +434,140 @@ def run_batched(args):
     return 0
 
 
+def serve_requests(n, seed=0, sizes=(8, 48)):
+    """The served stream: cubic boxes m^3, m uniform over sizes; nodes
+    perturbed +-0.05h; viscosity 1 with 8 seeded inclusions (radius 0.1), four
+    at c^(1/2) and four at c^(-1/2), c log-uniform in [1e2, 1e6]; free-slip box
+    BCs; f uniform [-1, 1] on free dofs."""
+    from pt_b200 import mesh as M
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(n):
+        m = int(rng.integers(sizes[0], sizes[1] + 1))
+        c = 10.0 ** rng.uniform(2.0, 6.0)
+        mesh = M.make_mesh(m, m, m, perturb=0.05, seed=seed * 1000003 + i)
+        r = np.random.default_rng(seed * 7919 + i + 1)
+        centres = r.uniform(0.0, 1.0, size=(8, 3))
+        vals = [c ** 0.5] * 4 + [c ** -0.5] * 4
+        eta = M.eta_spheres(mesh, centres, [0.1] * 8, vals)
+        mask = M.bc_mask_freeslip(m, m, m)
+        f = M_uniform(mesh.nvel, seed * 31 + i)
+        f[mask.astype(bool)] = 0.0
+        out.append((mesh, eta, mask, f, c))
+    return out
+
+
+def serve_run(reqs, arrivals, iters, **opts):
+    """Serve reqs arriving at the given times (seconds on the server clock,
+    relative to the first arrival).  Returns (results by id, stats)."""
+    from pt_b200.serve import Server
+    res, max_active, max_bytes = {}, 0, 0
+    with Server(**opts) as s:
+        t0 = s.time()
+        nxt = 0
+        while len(res) < len(reqs):
+            now = s.time() - t0
+            while nxt < len(reqs) and arrivals[nxt] <= now:
+                m, eta, mask, f, _ = reqs[nxt]
+                s.submit(nxt, m.dims, m.coords, eta, mask, f)
+                nxt += 1
+            act, queued = s.step(iters)
+            max_active = max(max_active, act)
+            max_bytes = max(max_bytes, s.stats()["bytes_in_use"])
+            for d in s.done():
+                d["t_done"] -= t0
+                d["t_submit"] -= t0
+                d["t_admit"] -= t0
+                res[d["id"]] = d
+            if act == 0 and queued == 0 and nxt < len(reqs):
+                time.sleep(max(0.0, min(0.01, arrivals[nxt] - (s.time() - t0))))
+        st = s.stats()
+    st.update(max_active=max_active, max_bytes_in_use=max_bytes)
+    return res, st
+
+
+def run_serve(args):
+    """Serving form: Poisson arrivals at ~80% of the measured capacity, solves
+    of A11 u = f to rtol 1e-8 by FP32 Chebyshev(3)-Jacobi-preconditioned FP64
+    CG, continuously batched; p50/p99 latency and solves/s against serial
+    plain FP64 solves of the same requests."""
+    import torch
+
+    from pt_b200 import MatStokesMF
+    from pt_b200.solver import KSPSolveA11
+    torch.cuda.set_device(0)
+    t_gen = time.time()
+    cal = serve_requests(args.ncal, seed=1)
+    reqs = serve_requests(args.nreq, seed=0)
+    t_gen = time.time() - t_gen
+    # tile schedule (tile width, z-chunk depth) by the autotuner, on the
+    # calibration requests' FP32 applies
+    from pt_b200.batch import autotune
+    ops = []
+    for m, eta, mask, _, _ in cal:
+        op = MatStokesMF(*m.dims)
+        op.SetUp(m.coords, eta, mask)
+        ops.append(op)
+    us = [torch.ones(op.nvel, dtype=torch.float32, device="cuda") for op in ops]
+    ys = [torch.empty_like(u) for u in us]
+    (lz, tile_x), table = autotune(ops, us, ys, lz_candidates=(1, 2, 0), tile_candidates=(0, 64, 128))
+    for op in ops:
+        op.Destroy()
+    opts = dict(rtol=args.rtol, max_it=args.max_it, cheby_fp32=1, cheby_degree=args.cheby_degree,
+                memory_budget_bytes=120 << 30, max_active=256, lz=lz, tile_x=tile_x)
+    # capacity: a saturated queue (everything arrives at once)
+    res_cal, _ = serve_run(cal, [0.0] * len(cal), args.serve_iters, **opts)
+    capacity = len(cal) / max(d["t_done"] for d in res_cal.values())
+    rate = 0.8 * capacity
+    rng = np.random.default_rng(12345)
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, size=len(reqs)))
+    arrivals -= arrivals[0]
+    res, st = serve_run(reqs, arrivals, args.serve_iters, **opts)
+    lat = np.array([res[i]["t_done"] - arrivals[i] for i in range(len(reqs))])
+    wall = max(d["t_done"] for d in res.values())
+    its = np.array([res[i]["its"] for i in range(len(reqs))])
+    conv = all(res[i]["converged"] for i in range(len(reqs)))
+    # true FP64 residual of a sample of served results
+    relres = []
+    for i in range(0, len(reqs), max(1, len(reqs) // 8)):
+        m, eta, mask, f, _ = reqs[i]
+        with MatStokesMF(*m.dims) as op:
+            op.SetUp(m.coords, eta, mask)
+            y = op.MatMult_MFStokes_A11(torch.from_numpy(res[i]["x"]).cuda()).cpu().numpy()
+        relres.append(float(np.linalg.norm(f - y) / np.linalg.norm(f)))
+    # serial plain FP64 solves (one request at a time, set-up included)
+    serial = []
+    for i in np.linspace(0, len(reqs) - 1, min(args.nserial, len(reqs))).astype(int):
+        m, eta, mask, f, _ = reqs[i]
+        torch.cuda.synchronize()
+        t = time.time()
+        with MatStokesMF(*m.dims) as op:
+            op.SetUp(m.coords, eta, mask)
+            fd = torch.from_numpy(f).cuda()
+            x = torch.zeros_like(fd)
+            with KSPSolveA11(op, ksp="fcg", pc="cheby_jacobi", cheby_fp32=0, cheby_degree=args.cheby_degree,
+                             rtol=args.rtol, max_it=args.max_it) as k:
+                sst = k.solve(fd, x)
+            x.cpu()
+        serial.append({"seconds": time.time() - t, "its": sst["its"], "converged": sst["converged"],
+                       "elements": m.nel, "served_its": res[int(i)]["its"]})
+    serial_rate = len(serial) / sum(d["seconds"] for d in serial)
+    out = {"mode": "serve", "requests": len(reqs), "sizes": "m^3, m uniform 8..48",
+           "contrast": "log-uniform [1e2, 1e6]", "rtol": args.rtol, "iterations_per_step": args.serve_iters,
+           "capacity_solves_per_s": capacity, "arrival_rate_per_s": rate, "calibration_requests": len(cal),
+           "solves_per_s": len(reqs) / wall, "p50_latency_s": float(np.percentile(lat, 50)),
+           "p99_latency_s": float(np.percentile(lat, 99)), "mean_its": float(its.mean()),
+           "max_its": int(its.max()), "all_converged": conv, "true_relres_sample_max": max(relres),
+           "serial_fp64_solves_per_s": serial_rate, "serial_sample": len(serial),
+           "serial_mean_its": float(np.mean([d["its"] for d in serial])),
+           "serial_mean_served_its_same_requests": float(np.mean([d["served_its"] for d in serial])),
+           "speedup_solves_per_s": (len(reqs) / wall) / serial_rate, "server": st,
+           "autotune": {"lz": lz, "tile_x": tile_x, "ms": {f"lz{a}_tx{b}": v for (a, b), v in table.items()}},
+           "host_generation_s": t_gen}
+    print(json.dumps(out))
+    return 0
+
+
 def M_uniform(n, seed):
     return np.random.default_rng(seed).uniform(-1.0, 1.0, size=n)
 
@@ -449,7 +583,11 @@ def main():
     ap.add_argument("--quick", action="store_true", help="headline A11 only")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
-    ap.add_argument("--mode", default="apply", choices=["apply", "solve", "batched"])
+    ap.add_argument("--mode", default="apply", choices=["apply", "solve", "batched", "serve"])
+    ap.add_argument("--nreq", type=int, default=200, help="serve: requests in the measured stream")
+    ap.add_argument("--ncal", type=int, default=48, help="serve: requests of the capacity calibration")
+    ap.add_argument("--nserial", type=int, default=12, help="serve: requests solved one at a time")
+    ap.add_argument("--serve-iters", type=int, default=8, help="serve: iterations per server step")
     ap.add_argument("--nbatch", type=int, default=256)
     ap.add_argument("--ksp", default="fgmres")
     ap.add_argument("--rtol", type=float, default=1e-8)
@@ -462,6 +600,8 @@ def main():
         return run_solve(args)
     if args.mode == "batched":
         return run_batched(args)
+    if args.mode == "serve":
+        return run_serve(args)
     if args.impl == "reference":
         return run_reference(args)
     return run_ours(args)

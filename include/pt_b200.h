@@ -242,6 +242,10 @@ pt_status pt_solver_destroy(pt_solver *solver);
  * the autotuner in pt_b200/batch.py picks it. */
 typedef struct pt_batch pt_batch;
 pt_status pt_batch_create(int n, pt_op *const *ops, const int32_t *lz, pt_batch **batch);
+/* As pt_batch_create with every box tiled tile_x elements wide (32, 64 or
+ * 128; 0 = each box's own width).  One width for all boxes puts the whole
+ * batch in one class per colour, fewer launches per apply. */
+pt_status pt_batch_create_tiled(int n, pt_op *const *ops, const int32_t *lz, int32_t tile_x, pt_batch **batch);
 pt_status pt_batch_destroy(pt_batch *batch);
 int64_t pt_batch_launches_per_apply(const pt_batch *batch);
 int64_t pt_batch_tiles(const pt_batch *batch);
@@ -264,6 +268,7 @@ typedef struct {
   int64_t memory_budget_bytes; /* device bytes for admitted requests (default 120 GiB) */
   int32_t max_active;          /* requests iterated together (default 256) */
   int32_t lz;                  /* element layers per z-chunk of the A11 tiles (0: per-box default) */
+  int32_t tile_x;              /* A11 tile width for every request (32/64/128; 0: per box; default 64) */
   int32_t cheby_fp32, cheby_degree;
   double cheby_emin, cheby_emax;
   int32_t eig_its;
@@ -298,6 +303,9 @@ pt_status pt_server_step(pt_server *server, int32_t iterations, int32_t *n_activ
 /* Next finished request (res->id = -1 when none). */
 pt_status pt_server_next_done(pt_server *server, pt_server_result *res);
 pt_status pt_server_stats(const pt_server *server, int64_t *iterations, int64_t *launches, int64_t *bytes_in_use);
+/* Host seconds spent enqueueing iterations (incl. batch rebuilds), admitting,
+ * waiting for the device, and retiring. */
+pt_status pt_server_timers(const pt_server *server, double *enqueue, double *admit, double *wait, double *retire);
 
 /* ---- selection, in the style of -a11_op --------------------------------- */
 

@@ -67,9 +67,11 @@ pt_status batch_apply(pt_batch *b, const T *const *u, T *const *y, void *stream)
 
 extern "C" {
 
-pt_status pt_batch_create(int n, pt_op *const *ops, const int32_t *lz, pt_batch **out)
+pt_status pt_batch_create_tiled(int n, pt_op *const *ops, const int32_t *lz, int32_t tile_x, pt_batch **out)
 {
   if (!out || n < 1 || !ops) return fail(PT_ERR_BAD_ARG, "need n >= 1 ops");
+  if (tile_x != 0 && tile_x != 32 && tile_x != 64 && tile_x != 128)
+    return fail(PT_ERR_BAD_ARG, "tile_x must be 0, 32, 64 or 128");
   *out = nullptr;
   std::vector<ptk::BatchProb> p64(n), p32(n);
   // class key: (pass, TX) -> items
@@ -82,9 +84,11 @@ pt_status pt_batch_create(int n, pt_op *const *ops, const int32_t *lz, pt_batch 
     if (!op->full_box) return fail(PT_ERR_UNSUPPORTED, "batch problem %d: one-rank boxes only", i);
     if ((s = ensure_geometry(op)) != PT_OK) return s;
     if (!op->geom_ok) return fail(PT_ERR_BAD_ARG, "batch problem %d has w*eta/detJ <= 0 somewhere", i);
+    // any tile width covers the box: tiles read K columns ex < mx <= MXP
+    const int TX = tile_x ? tile_x : op->TX;
     ptk::BatchProb d;
     d.b = op->box;
-    d.ntx = op->ntx;
+    d.ntx = (op->mx + TX - 1) / TX;
     d.MXP = op->MXP;
     int L = (lz && lz[i] > 0) ? lz[i] : op->LZ;
     if (L > op->mz) L = op->mz;
@@ -99,7 +103,7 @@ pt_status pt_batch_create(int n, pt_op *const *ops, const int32_t *lz, pt_batch 
       for (int ej = 0; ej < op->my; ej++)
         for (int tx = 0; tx < d.ntx; tx++) {
           const int pass = (tx & 1) + 2 * (ej & 1) + 4 * (zc & 1);
-          cls[{pass, op->TX}].push_back(make_int4(i, tx, ej, zc));
+          cls[{pass, TX}].push_back(make_int4(i, tx, ej, zc));
           tiles++;
         }
   }
@@ -132,6 +136,11 @@ pt_status pt_batch_create(int n, pt_op *const *ops, const int32_t *lz, pt_batch 
   }
   *out = b;
   return PT_OK;
+}
+
+pt_status pt_batch_create(int n, pt_op *const *ops, const int32_t *lz, pt_batch **out)
+{
+  return pt_batch_create_tiled(n, ops, lz, 0, out);
 }
 
 pt_status pt_batch_destroy(pt_batch *b)

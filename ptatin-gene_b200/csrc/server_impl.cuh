@@ -281,6 +281,7 @@ struct pt_server {
   int64_t nitems = 0;
   void *d_ptrs = nullptr;     // p[], q[], z[], az[] tables of the batch
   int64_t iterations = 0, launches = 0;
+  double t_enqueue = 0.0, t_admit = 0.0, t_wait = 0.0, t_retire = 0.0;  // host seconds per phase
   std::chrono::steady_clock::time_point t0;
   double now() const { return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count(); }
 };
@@ -477,7 +478,7 @@ pt_status srv_rebuild(pt_server *s)
   std::vector<void *> tab;
   const int na = (int)s->act.size();
   for (int i : s->act) ops.push_back(s->slots[i]->op);
-  pt_status e = pt_batch_create(na, ops.data(), nullptr, &s->batch);
+  pt_status e = pt_batch_create_tiled(na, ops.data(), nullptr, s->o.tile_x, &s->batch);
   if (e != PT_OK) return e;
   const size_t ts = s->fp32 ? sizeof(float) : sizeof(double);
   tab.resize(4 * na);
@@ -560,6 +561,7 @@ void pt_server_opts_default(pt_server_opts *o)
   o->memory_budget_bytes = (int64_t)120 << 30;
   o->max_active = 256;
   o->lz = 0;
+  o->tile_x = 64;
   o->cheby_fp32 = 1;
   o->cheby_degree = 3;
   o->cheby_emin = 0.2;
@@ -580,6 +582,8 @@ pt_status pt_server_create(const pt_server_opts *opts, pt_server **out)
   if (!(opts->cheby_emin > 0.0) || !(opts->cheby_emax > opts->cheby_emin))
     return fail(PT_ERR_BAD_ARG, "need 0 < cheby_emin < cheby_emax");
   if (opts->memory_budget_bytes <= 0) return fail(PT_ERR_BAD_ARG, "memory budget must be positive");
+  if (opts->tile_x != 0 && opts->tile_x != 32 && opts->tile_x != 64 && opts->tile_x != 128)
+    return fail(PT_ERR_BAD_ARG, "tile_x must be 0, 32, 64 or 128");
   pt_server *s = new (std::nothrow) pt_server();
   if (!s) return fail(PT_ERR_OOM, "host allocation failed");
   s->o = *opts;
@@ -657,6 +661,7 @@ pt_status pt_server_step(pt_server *s, int32_t iterations, int32_t *n_active, in
 {
   if (!s || iterations < 0) return fail(PT_ERR_BAD_ARG, "bad argument");
   pt_status e;
+  double tp = s->now();
   if (s->dirty && (e = srv_rebuild(s)) != PT_OK) return e;
   // 1. iterations of the current batch, enqueued (no host wait)
   if (!s->act.empty())
@@ -664,6 +669,9 @@ pt_status pt_server_step(pt_server *s, int32_t iterations, int32_t *n_active, in
       e = s->fp32 ? srv_iterate<float>(s) : srv_iterate<double>(s);
       if (e != PT_OK) return e;
     }
+  double tq = s->now();
+  s->t_enqueue += tq - tp;
+  tp = tq;
   // 2. admissions while they run: FIFO, as slots and the budget allow
   while (!s->queue.empty()) {
     SrvReq *r = s->queue.front();
@@ -685,9 +693,16 @@ pt_status pt_server_step(pt_server *s, int32_t iterations, int32_t *n_active, in
     }
     s->dirty = true;
   }
+  tq = s->now();
+  s->t_admit += tq - tp;
+  tp = tq;
   // 3. wait for the batch, retire finished requests
   PT_CUDA(cudaStreamSynchronize(s->main));
+  tq = s->now();
+  s->t_wait += tq - tp;
+  tp = tq;
   if ((e = srv_retire(s)) != PT_OK) return e;
+  s->t_retire += s->now() - tp;
   if (n_active) {
     int na = 0;
     for (SrvReq *r : s->slots) na += r != nullptr;
@@ -717,6 +732,16 @@ pt_status pt_server_next_done(pt_server *s, pt_server_result *res)
   res->t_admit = r->t_admit;
   res->t_done = r->t_done;
   delete r;
+  return PT_OK;
+}
+
+pt_status pt_server_timers(const pt_server *s, double *enqueue, double *admit, double *wait, double *retire)
+{
+  if (!s) return fail(PT_ERR_BAD_ARG, "NULL argument");
+  if (enqueue) *enqueue = s->t_enqueue;
+  if (admit) *admit = s->t_admit;
+  if (wait) *wait = s->t_wait;
+  if (retire) *retire = s->t_retire;
   return PT_OK;
 }
 

@@ -44,7 +44,7 @@ class SolveStats(ctypes.Structure):
 
 class ServerOpts(ctypes.Structure):
     _fields_ = [("memory_budget_bytes", ctypes.c_int64), ("max_active", ctypes.c_int32), ("lz", ctypes.c_int32),
-                ("cheby_fp32", ctypes.c_int32), ("cheby_degree", ctypes.c_int32),
+                ("tile_x", ctypes.c_int32), ("cheby_fp32", ctypes.c_int32), ("cheby_degree", ctypes.c_int32),
                 ("cheby_emin", ctypes.c_double), ("cheby_emax", ctypes.c_double), ("eig_its", ctypes.c_int32),
                 ("rtol", ctypes.c_double), ("atol", ctypes.c_double), ("max_it", ctypes.c_int32)]
 
@@ -97,6 +97,7 @@ SIGNATURES = {
     "pt_solver_apply_pc_d": [_vp, _vp, _vp],
     "pt_solver_destroy": [_vp],
     "pt_batch_create": [ctypes.c_int, _vp, _vp, ctypes.POINTER(_vp)],
+    "pt_batch_create_tiled": [ctypes.c_int, _vp, _vp, ctypes.c_int32, ctypes.POINTER(_vp)],
     "pt_batch_destroy": [_vp],
     "pt_batch_launches_per_apply": [_vp],
     "pt_batch_tiles": [_vp],
@@ -110,6 +111,8 @@ SIGNATURES = {
     "pt_server_step": [_vp, ctypes.c_int32, _i32p, _i32p],
     "pt_server_next_done": [_vp, ctypes.POINTER(ServerResult)],
     "pt_server_stats": [_vp, _i64p, _i64p, _i64p],
+    "pt_server_timers": [_vp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double),
+                         ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)],
     "pt_op_set_a11_kernel": [_vp, ctypes.c_char_p],
     "pt_op_get_a11_kernel": [_vp],
     "pt_op_launch_count": [_vp],

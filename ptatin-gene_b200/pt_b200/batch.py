@@ -18,7 +18,7 @@ def _ptr_table(tensors, device):
 
 
 class BatchA11:
-    def __init__(self, ops, lz=None):
+    def __init__(self, ops, lz=None, tile_x=0):
         self.ops = list(ops)
         n = len(self.ops)
         arr = (ctypes.c_void_p * n)(*[op.handle.value for op in self.ops])
@@ -27,7 +27,7 @@ class BatchA11:
             vals = [int(lz)] * n if isinstance(lz, int) else [int(v) for v in lz]
             lzs = (ctypes.c_int32 * n)(*vals)
         h = ctypes.c_void_p()
-        _capi.call("pt_batch_create", n, arr, lzs, ctypes.byref(h))
+        _capi.call("pt_batch_create_tiled", n, arr, lzs, int(tile_x), ctypes.byref(h))
         self._h = h
         self._tables = {}
         lib = _capi.load()
@@ -75,18 +75,33 @@ def autotune_lz(ops, us, ys, candidates=(1, 2, 4, 8, 0), reps=3, masked=True):
     """Pick the z-chunk depth (element layers per tile; 0 = each op's default)
     that makes one batched apply fastest on these problems.  Returns
     (best_lz, {lz: ms})."""
+    best, times = autotune(ops, us, ys, lz_candidates=candidates, tile_candidates=(0,), reps=reps, masked=masked)
+    return best[0], {lz: t for (lz, _), t in times.items()}
+
+
+def autotune(ops, us, ys, lz_candidates=(1, 2, 4, 0), tile_candidates=(0, 64), reps=3, masked=True):
+    """Pick the tile schedule -- z-chunk depth (element layers per tile; 0 =
+    each op's default) and tile width (0 = each op's own) -- that makes one
+    batched apply fastest on these problems.  Returns ((lz, tile_x),
+    {(lz, tile_x): ms})."""
     import torch
     times = {}
-    for lz in candidates:
-        with BatchA11(ops, lz=lz if lz else None) as b:
-            b.apply(us, ys, masked)
-            torch.cuda.synchronize()
-            ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            ev0.record()
-            for _ in range(reps):
-                b.apply(us, ys, masked)
-            ev1.record()
-            ev1.synchronize()
-            times[lz] = ev0.elapsed_time(ev1) / reps
+    for lz in lz_candidates:
+        for tx in tile_candidates:
+            times[(lz, tx)] = _time_batch(ops, us, ys, lz, tx, reps, masked, torch)
     best = min(times, key=times.get)
     return best, times
+
+
+def _time_batch(ops, us, ys, lz, tile_x, reps, masked, torch):
+    """Mean ms of one batched apply under a schedule (CUDA events)."""
+    with BatchA11(ops, lz=lz if lz else None, tile_x=tile_x) as b:
+        b.apply(us, ys, masked)
+        torch.cuda.synchronize()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record()
+        for _ in range(reps):
+            b.apply(us, ys, masked)
+        ev1.record()
+        ev1.synchronize()
+        return ev0.elapsed_time(ev1) / reps

@@ -79,7 +79,10 @@ class Server:
     def stats(self):
         it, la, by = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64()
         _capi.call("pt_server_stats", self._h, ctypes.byref(it), ctypes.byref(la), ctypes.byref(by))
-        return {"iterations": it.value, "launches": la.value, "bytes_in_use": by.value}
+        t = [ctypes.c_double() for _ in range(4)]
+        _capi.call("pt_server_timers", self._h, *[ctypes.byref(v) for v in t])
+        return {"iterations": it.value, "launches": la.value, "bytes_in_use": by.value,
+                "host_s": {k: v.value for k, v in zip(("enqueue", "admit", "wait", "retire"), t)}}
 
     def destroy(self):
         if getattr(self, "_h", None):
