@@ -74,6 +74,10 @@ class ClockSampler:
                  "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self._t = threading.Thread(target=self._read, daemon=True)
             self._t.start()
+            # the timed region starts once samples flow
+            t_end = time.time() + 3.0
+            while not self.lines and time.time() < t_end:
+                time.sleep(0.01)
         except Exception:
             self.proc = None
         return self
@@ -575,7 +579,7 @@ def M_uniform(n, seed):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="c2")
