@@ -22,6 +22,11 @@ struct pt_batch {
   };
   std::vector<Cls> classes;
   int64_t tiles;
+  // pooled (server) batches: stream-ordered buffers; host copies kept until destroy
+  cudaMemPool_t pool;
+  cudaStream_t stream;
+  std::vector<ptk::BatchProb> h64, h32;
+  std::vector<int4> hitems;
 };
 
 namespace {
@@ -67,7 +72,10 @@ pt_status batch_apply(pt_batch *b, const T *const *u, T *const *y, void *stream)
 
 extern "C" {
 
-pt_status pt_batch_create_tiled(int n, pt_op *const *ops, const int32_t *lz, int32_t tile_x, pt_batch **out)
+// pool == null: cudaMalloc + synchronous upload; else buffers from `pool`
+// with asynchronous uploads, both ordered on `stream`.
+static pt_status batch_create_impl(int n, pt_op *const *ops, const int32_t *lz, int32_t tile_x, cudaMemPool_t pool,
+                                   cudaStream_t stream, pt_batch **out)
 {
   if (!out || n < 1 || !ops) return fail(PT_ERR_BAD_ARG, "need n >= 1 ops");
   if (tile_x != 0 && tile_x != 32 && tile_x != 64 && tile_x != 128)
@@ -112,7 +120,9 @@ pt_status pt_batch_create_tiled(int n, pt_op *const *ops, const int32_t *lz, int
   b->n = n;
   b->ops.assign(ops, ops + n);
   b->tiles = tiles;
-  std::vector<int4> all;
+  b->pool = pool;
+  b->stream = stream;
+  std::vector<int4> &all = b->hitems;
   for (auto &kv : cls) {
     pt_batch::Cls c;
     c.px = kv.first.first & 1; c.py = (kv.first.first >> 1) & 1; c.pz = (kv.first.first >> 2) & 1;
@@ -122,12 +132,25 @@ pt_status pt_batch_create_tiled(int n, pt_op *const *ops, const int32_t *lz, int
     all.insert(all.end(), kv.second.begin(), kv.second.end());
     b->classes.push_back(c);
   }
-  cudaError_t e = cudaMalloc(&b->d_probs64, sizeof(ptk::BatchProb) * n);
-  if (e == cudaSuccess) e = cudaMalloc(&b->d_probs32, sizeof(ptk::BatchProb) * n);
-  if (e == cudaSuccess) e = cudaMalloc(&b->d_items, sizeof(int4) * all.size());
-  if (e == cudaSuccess) e = cudaMemcpy(b->d_probs64, p64.data(), sizeof(ptk::BatchProb) * n, cudaMemcpyHostToDevice);
-  if (e == cudaSuccess) e = cudaMemcpy(b->d_probs32, p32.data(), sizeof(ptk::BatchProb) * n, cudaMemcpyHostToDevice);
-  if (e == cudaSuccess) e = cudaMemcpy(b->d_items, all.data(), sizeof(int4) * all.size(), cudaMemcpyHostToDevice);
+  b->h64 = p64;
+  b->h32 = p32;
+  cudaError_t e;
+  const size_t bp = sizeof(ptk::BatchProb) * n, bi = sizeof(int4) * all.size();
+  if (pool) {
+    e = cudaMallocFromPoolAsync((void **)&b->d_probs64, bp, pool, stream);
+    if (e == cudaSuccess) e = cudaMallocFromPoolAsync((void **)&b->d_probs32, bp, pool, stream);
+    if (e == cudaSuccess) e = cudaMallocFromPoolAsync((void **)&b->d_items, bi, pool, stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(b->d_probs64, b->h64.data(), bp, cudaMemcpyHostToDevice, stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(b->d_probs32, b->h32.data(), bp, cudaMemcpyHostToDevice, stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(b->d_items, all.data(), bi, cudaMemcpyHostToDevice, stream);
+  } else {
+    e = cudaMalloc(&b->d_probs64, bp);
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_probs32, bp);
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_items, bi);
+    if (e == cudaSuccess) e = cudaMemcpy(b->d_probs64, p64.data(), bp, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(b->d_probs32, p32.data(), bp, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(b->d_items, all.data(), bi, cudaMemcpyHostToDevice);
+  }
   if (e != cudaSuccess) {
     pt_status s = fail(e == cudaErrorMemoryAllocation ? PT_ERR_OOM : PT_ERR_CUDA, "pt_batch_create: %s",
                        cudaGetErrorString(e));
@@ -138,17 +161,25 @@ pt_status pt_batch_create_tiled(int n, pt_op *const *ops, const int32_t *lz, int
   return PT_OK;
 }
 
+pt_status pt_batch_create_tiled(int n, pt_op *const *ops, const int32_t *lz, int32_t tile_x, pt_batch **out)
+{
+  return batch_create_impl(n, ops, lz, tile_x, nullptr, nullptr, out);
+}
+
 pt_status pt_batch_create(int n, pt_op *const *ops, const int32_t *lz, pt_batch **out)
 {
-  return pt_batch_create_tiled(n, ops, lz, 0, out);
+  return batch_create_impl(n, ops, lz, 0, nullptr, nullptr, out);
 }
 
 pt_status pt_batch_destroy(pt_batch *b)
 {
   if (!b) return PT_OK;
-  cudaFree(b->d_probs64);
-  cudaFree(b->d_probs32);
-  cudaFree(b->d_items);
+  void *bufs[] = {b->d_probs64, b->d_probs32, b->d_items};
+  for (void *p : bufs) {
+    if (!p) continue;
+    if (b->pool) cudaFreeAsync(p, b->stream);
+    else cudaFree(p);
+  }
   delete b;
   return PT_OK;
 }

@@ -80,9 +80,25 @@ struct pt_op {
   int64_t launches;
   uint64_t state;  // bumped whenever coordinates, viscosity or the mask change
   int device;
+  cudaMemPool_t pool;  // non-null: buffers are stream-ordered allocations from this pool on `stream`
 };
 
 namespace {
+
+// Device buffers of an op: cudaMalloc, or stream-ordered from the op's pool
+// (no device-wide synchronisation on free; used by the request server).
+cudaError_t op_alloc(pt_op *op, void **p, size_t bytes)
+{
+  if (op->pool) return cudaMallocFromPoolAsync(p, bytes, op->pool, op->stream);
+  return cudaMalloc(p, bytes);
+}
+
+void op_free(pt_op *op, void *p)
+{
+  if (!p) return;
+  if (op->pool) cudaFreeAsync(p, op->stream);
+  else cudaFree(p);
+}
 
 constexpr int TPB = 128;
 
@@ -242,9 +258,9 @@ pt_status ensure_geometry(pt_op *op)
   if (!op->geom_dirty) return PT_OK;
   const int64_t nk = (int64_t)op->my * op->mz * 243 * op->MXP;
   if (!op->d_K) {
-    PT_CUDA(cudaMalloc(&op->d_K, sizeof(double) * nk));
-    PT_CUDA(cudaMalloc(&op->d_K32, sizeof(float) * nk));
-    PT_CUDA(cudaMalloc(&op->d_bad, sizeof(unsigned int)));
+    PT_CUDA(op_alloc(op, (void **)&op->d_K, sizeof(double) * nk));
+    PT_CUDA(op_alloc(op, (void **)&op->d_K32, sizeof(float) * nk));
+    PT_CUDA(op_alloc(op, (void **)&op->d_bad, sizeof(unsigned int)));
   }
   PT_CUDA(cudaMemsetAsync(op->d_bad, 0, sizeof(unsigned int), op->stream));
   ptk::geom_kernel<double><<<nblocks(op->nel), TPB, 0, op->stream>>>(op->box, op->MXP, op->d_coords, op->d_eta,
@@ -398,7 +414,9 @@ extern "C" {
 const char *pt_last_error(void) { return g_err.c_str(); }
 const char *pt_version(void) { return "pt_b200 0.1 (sm_100a)"; }
 
-pt_status pt_op_create(const pt_mesh_desc *desc, pt_op **out)
+// pool == null: pt_op_create (own stream, cudaMalloc).  Otherwise every
+// buffer comes from `pool`, ordered on `stream`, which the op then uses.
+static pt_status op_create_impl(const pt_mesh_desc *desc, cudaMemPool_t pool, cudaStream_t stream, pt_op **out)
 {
   if (!desc || !out) return fail(PT_ERR_BAD_ARG, "NULL argument");
   *out = nullptr;
@@ -440,14 +458,20 @@ pt_status pt_op_create(const pt_mesh_desc *desc, pt_op **out)
                  (nz == 2 * (int64_t)desc->mz + 1);
   op->geom_dirty = true;
   cudaError_t e = cudaGetDevice(&op->device);
-  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&op->stream, cudaStreamNonBlocking);
-  if (e == cudaSuccess) op->own_stream = true;
-  if (e == cudaSuccess) e = cudaMalloc(&op->d_coords, sizeof(double) * op->nvel);
-  if (e == cudaSuccess) e = cudaMalloc(&op->d_eta, sizeof(double) * 27 * op->nel);
-  if (e == cudaSuccess) e = cudaMalloc(&op->d_coords32, sizeof(float) * op->nvel);
-  if (e == cudaSuccess) e = cudaMalloc(&op->d_eta32, sizeof(float) * 27 * op->nel);
-  if (e == cudaSuccess) e = cudaMalloc(&op->d_mask, op->nvel);
-  if (e == cudaSuccess) e = cudaMemset(op->d_mask, 0, op->nvel);
+  if (pool) {
+    op->pool = pool;
+    op->stream = stream;
+  } else {
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&op->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) op->own_stream = true;
+  }
+  if (e == cudaSuccess) e = op_alloc(op, (void **)&op->d_coords, sizeof(double) * op->nvel);
+  if (e == cudaSuccess) e = op_alloc(op, (void **)&op->d_eta, sizeof(double) * 27 * op->nel);
+  if (e == cudaSuccess) e = op_alloc(op, (void **)&op->d_coords32, sizeof(float) * op->nvel);
+  if (e == cudaSuccess) e = op_alloc(op, (void **)&op->d_eta32, sizeof(float) * 27 * op->nel);
+  if (e == cudaSuccess) e = op_alloc(op, (void **)&op->d_mask, op->nvel);
+  if (e == cudaSuccess) e = cudaMemsetAsync(op->d_mask, 0, op->nvel, op->stream);
+  if (e == cudaSuccess && !pool) e = cudaStreamSynchronize(op->stream);
   if (e != cudaSuccess) {
     pt_status s = fail(e == cudaErrorMemoryAllocation ? PT_ERR_OOM : PT_ERR_CUDA, "pt_op_create: %s",
                        cudaGetErrorString(e));
@@ -458,15 +482,16 @@ pt_status pt_op_create(const pt_mesh_desc *desc, pt_op **out)
   return PT_OK;
 }
 
+pt_status pt_op_create(const pt_mesh_desc *desc, pt_op **out) { return op_create_impl(desc, nullptr, nullptr, out); }
+
 pt_status pt_op_destroy(pt_op *op)
 {
   if (!op) return PT_OK;
-  if (op->stream) cudaStreamSynchronize(op->stream);
-  cudaFree(op->d_coords); cudaFree(op->d_eta);
-  cudaFree(op->d_coords32); cudaFree(op->d_eta32);
-  cudaFree(op->d_mask);
-  cudaFree(op->d_u); cudaFree(op->d_y); cudaFree(op->d_p);
-  cudaFree(op->d_K); cudaFree(op->d_K32); cudaFree(op->d_bad);
+  // pooled ops free in stream order (after the op's queued work); others wait
+  if (op->stream && !op->pool) cudaStreamSynchronize(op->stream);
+  void *bufs[] = {op->d_coords, op->d_eta, op->d_coords32, op->d_eta32, op->d_mask, op->d_u,
+                  op->d_y, op->d_p, op->d_K, op->d_K32, op->d_bad};
+  for (void *b : bufs) op_free(op, b);
   if (op->own_stream && op->stream) cudaStreamDestroy(op->stream);
   free(op);
   return PT_OK;
@@ -577,9 +602,9 @@ pt_status pt_op_set_bc_mask_h(pt_op *op, const uint8_t *mask)
 
 static pt_status ensure_staging(pt_op *op)
 {
-  if (!op->d_u) PT_CUDA(cudaMalloc(&op->d_u, sizeof(double) * op->nvel));
-  if (!op->d_y) PT_CUDA(cudaMalloc(&op->d_y, sizeof(double) * op->nvel));
-  if (!op->d_p) PT_CUDA(cudaMalloc(&op->d_p, sizeof(double) * op->npres));
+  if (!op->d_u) PT_CUDA(op_alloc(op, (void **)&op->d_u, sizeof(double) * op->nvel));
+  if (!op->d_y) PT_CUDA(op_alloc(op, (void **)&op->d_y, sizeof(double) * op->nvel));
+  if (!op->d_p) PT_CUDA(op_alloc(op, (void **)&op->d_p, sizeof(double) * op->npres));
   return PT_OK;
 }
 

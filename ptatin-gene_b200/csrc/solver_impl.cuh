@@ -173,34 +173,36 @@ unsigned vgrid(int64_t n)
   return (unsigned)std::max<int64_t>(1, std::min<int64_t>(b, 148 * 8));
 }
 
-// Largest eigenvalue of a symmetric tridiagonal matrix (bisection on Sturm counts).
-double tridiag_lambda_max(const std::vector<double> &a, const std::vector<double> &b)
+// Largest eigenvalue of a symmetric tridiagonal matrix (diagonal a[0..n),
+// off-diagonal b[0..n-1)) by bisection on Sturm counts.  Host and device.
+__host__ __device__ inline double tridiag_lmax(const double *a, const double *b, int n)
 {
-  const int n = (int)a.size();
   if (n == 0) return 0.0;
   double lo = a[0], hi = a[0];
   for (int i = 0; i < n; i++) {
-    const double r = (i > 0 ? std::fabs(b[i - 1]) : 0.0) + (i + 1 < n ? std::fabs(b[i]) : 0.0);
-    lo = std::min(lo, a[i] - r);
-    hi = std::max(hi, a[i] + r);
+    const double r = (i > 0 ? fabs(b[i - 1]) : 0.0) + (i + 1 < n ? fabs(b[i]) : 0.0);
+    lo = fmin(lo, a[i] - r);
+    hi = fmax(hi, a[i] + r);
   }
-  auto count_below = [&](double x) {
+  for (int it = 0; it < 200; it++) {
+    const double mid = 0.5 * (lo + hi);
     int c = 0;
-    double q = a[0] - x;
+    double q = a[0] - mid;
     if (q < 0) c++;
     for (int i = 1; i < n; i++) {
       const double qq = (q == 0.0) ? 1e-300 : q;
-      q = a[i] - x - b[i - 1] * b[i - 1] / qq;
+      q = a[i] - mid - b[i - 1] * b[i - 1] / qq;
       if (q < 0) c++;
     }
-    return c;
-  };
-  for (int it = 0; it < 200; it++) {
-    const double mid = 0.5 * (lo + hi);
-    if (count_below(mid) >= n) hi = mid;
+    if (c >= n) hi = mid;
     else lo = mid;
   }
   return hi;
+}
+
+double tridiag_lambda_max(const std::vector<double> &a, const std::vector<double> &b)
+{
+  return tridiag_lmax(a.data(), b.data(), (int)a.size());
 }
 
 }  // namespace
