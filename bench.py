@@ -38,6 +38,19 @@ REPO = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(REPO, "ptatin-gene_b200"))
 
 METRIC = "Q2 A11 GDoF/s FP64 vs FP32 @128³; batched solves/s & p99 @rtol 1e-8"
+
+WORKLOAD_TEXT = {
+    "c2": "perturbed +-0.05h, layered eta + 64 inclusions (1e6 contrast)",
+    "c1": "undeformed, sinker eta (16 spheres r 0.08, 1e4)",
+    "c0": "perturbed +-0.1h, log-uniform Gauss-point eta [1e-2, 1e2]",
+    "box": "perturbed +-0.1h, log-uniform Gauss-point eta [1e-2, 1e2]",
+    "sinker": "perturbed +-0.05h, sinker eta",
+    "layered": "perturbed +-0.05h, layered eta + inclusions",
+}
+# DRAM bytes per element of one FP64 streaming apply (K 1.94 KB + u/y tiles),
+# measured with ncu on the 96^3 box: 2 colour launches averaged 0.730 GB for
+# 96^3/4 elements.
+TRAFFIC_PER_ELEMENT_F64 = 4 * 0.730e9 / 96 ** 3
 UNIT = "GDoF/s"
 
 
@@ -255,6 +268,11 @@ def run_ours(args):
         ev1.synchronize()
         return ev0.elapsed_time(ev1) / 1e3
 
+    # ---- tile schedule by the autotuner (untimed), then the headline --------
+    tiling = {"lz": op.tiling, "autotune": None}
+    if not args.no_autotune and args.a11_op in ("b200", "b200_tmem"):
+        best, table = op.autotune_tiling(x)
+        tiling = {"lz": best, "autotune_ms": {str(k): round(v, 4) for k, v in table.items()}}
     # ---- headline: FP64 A11 (MatShell level), device resident ----------------
     for _ in range(max(args.warmup, 3)):
         op.MatMult_MFStokes_A11(x, y)
@@ -316,12 +334,14 @@ def run_ours(args):
             "warmup": max(args.warmup, 3), "ms_per_step": t_apply * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": f"A11 FP64 MatMult, {m.mx}x{m.my}x{m.mz} Q2 box ({m.nvel} velocity dofs), "
-                                   f"perturbed +-0.05h, layered eta + 64 inclusions (1e6 contrast), free-slip BCs",
+                                   f"{WORKLOAD_TEXT.get(args.workload.split(':')[0], args.workload)}, free-slip BCs",
                        "global_batch": 1, "seq_len": 0, "parallelism": f"replicas{ws}",
-                       "a11_op": op.a11_op, "l2": "inputs larger than L2 (no flush)"},
+                       "a11_op": op.a11_op, "tiling": tiling, "l2": "inputs larger than L2 (no flush)"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind,
-                         "algorithmic_bytes_per_apply": bytes_alg},
+                         "frac": achieved / peak, "traffic": TRAFFIC_PER_ELEMENT_F64 * m.nel,
+                         "traffic_source": "ncu dram__bytes_read+write of the 4 colour launches of one 96^3 apply "
+                                           "(profiles/a11_stream_96cubed.md), scaled by the element count",
+                         "peak_kind": peak_kind, "algorithmic_bytes_per_apply": bytes_alg},
             "cpu_baseline": cpu,
             "e2e": e2e,
             "gpu_launches": launches,
@@ -586,6 +606,7 @@ def main():
     ap.add_argument("--a11-op", default="b200")
     ap.add_argument("--quick", action="store_true", help="headline A11 only")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true", help="apply: keep the default tile schedule")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--mode", default="apply", choices=["apply", "solve", "batched", "serve"])
     ap.add_argument("--nreq", type=int, default=200, help="serve: requests in the measured stream")

@@ -317,6 +317,12 @@ pt_status pt_server_timers(const pt_server *server, double *enqueue, double *adm
  * PT_ERR_BAD_ARG, as the reference's SETERRQ1 "No -a11_op %s". */
 pt_status pt_op_set_a11_kernel(pt_op *op, const char *name);
 const char *pt_op_get_a11_kernel(const pt_op *op);
+/* Tile schedule of the streaming kernel: element layers per z-chunk of a CTA
+ * (0 = the default, about 2048 tiles).  Changes the summation order, so
+ * results differ in the last bits between schedules (each is deterministic).
+ * No counterpart in the reference; set by the autotuner. */
+pt_status pt_op_set_tiling(pt_op *op, int32_t lz);
+int32_t pt_op_get_tiling(const pt_op *op);
 
 /* Device-side timing helpers: launch count of this library's kernels on this
  * op since the last reset (for benchmark accounting). */

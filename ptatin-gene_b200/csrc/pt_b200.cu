@@ -445,15 +445,7 @@ static pt_status op_create_impl(const pt_mesh_desc *desc, cudaMemPool_t pool, cu
   op->TX = desc->mx <= 32 ? 32 : (desc->mx <= 64 ? 64 : 128);
   op->ntx = (desc->mx + op->TX - 1) / op->TX;
   op->MXP = (int64_t)op->ntx * op->TX;
-  {
-    // about 2048 CTAs in total, at least 2 layers per z-chunk where possible
-    const int64_t txy = (int64_t)op->ntx * desc->my;
-    int nzc = (int)((2048 + txy - 1) / txy);
-    nzc = nzc < 1 ? 1 : (nzc > (desc->mz + 1) / 2 ? (desc->mz + 1) / 2 : nzc);
-    if (nzc < 1) nzc = 1;
-    op->LZ = (desc->mz + nzc - 1) / nzc;
-    op->nzc = (desc->mz + op->LZ - 1) / op->LZ;
-  }
+  pt_op_set_tiling(op, 0);
   op->full_box = (nx == 2 * (int64_t)desc->mx + 1) && (ny == 2 * (int64_t)desc->my + 1) &&
                  (nz == 2 * (int64_t)desc->mz + 1);
   op->geom_dirty = true;
@@ -771,6 +763,24 @@ pt_status pt_op_set_a11_kernel(pt_op *op, const char *name)
   else return fail(PT_ERR_BAD_ARG, "No -a11_op %s", name);
   return PT_OK;
 }
+
+pt_status pt_op_set_tiling(pt_op *op, int32_t lz)
+{
+  if (!op) return fail(PT_ERR_BAD_ARG, "op is NULL");
+  if (lz < 0) return fail(PT_ERR_BAD_ARG, "lz must be >= 0");
+  if (lz == 0) {  // the default: about 2048 CTAs, at least 2 layers per z-chunk where possible
+    const int64_t txy = (int64_t)op->ntx * op->my;
+    int nzc = (int)((2048 + txy - 1) / txy);
+    nzc = nzc < 1 ? 1 : (nzc > (op->mz + 1) / 2 ? (op->mz + 1) / 2 : nzc);
+    if (nzc < 1) nzc = 1;
+    lz = (op->mz + nzc - 1) / nzc;
+  }
+  op->LZ = lz < op->mz ? lz : op->mz;
+  op->nzc = (op->mz + op->LZ - 1) / op->LZ;
+  return PT_OK;
+}
+
+int32_t pt_op_get_tiling(const pt_op *op) { return op ? op->LZ : 0; }
 
 const char *pt_op_get_a11_kernel(const pt_op *op)
 {

@@ -114,6 +114,8 @@ SIGNATURES = {
     "pt_server_timers": [_vp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double),
                          ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)],
     "pt_op_set_a11_kernel": [_vp, ctypes.c_char_p],
+    "pt_op_set_tiling": [_vp, ctypes.c_int32],
+    "pt_op_get_tiling": [_vp],
     "pt_op_get_a11_kernel": [_vp],
     "pt_op_launch_count": [_vp],
     "pt_op_reset_launch_count": [_vp],
@@ -131,6 +133,7 @@ _RESTYPES = {
     "pt_batch_tiles": ctypes.c_int64,
     "pt_server_opts_default": None,
     "pt_server_time": ctypes.c_double,
+    "pt_op_get_tiling": ctypes.c_int32,
 }
 
 _lib = None

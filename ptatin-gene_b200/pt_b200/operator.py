@@ -102,6 +102,41 @@ class MatStokesMF:
     def a11_op(self) -> str:
         return self._lib.pt_op_get_a11_kernel(self._h).decode()
 
+    def set_tiling(self, lz: int):
+        """Element layers per z-chunk of the streaming kernel's tiles (0 = default)."""
+        _capi.call("pt_op_set_tiling", self._h, int(lz))
+
+    @property
+    def tiling(self) -> int:
+        return int(self._lib.pt_op_get_tiling(self._h))
+
+    def autotune_tiling(self, X, candidates=(0, 2, 3, 4, 5, 6, 7, 8, 10, 12, 16), reps=5):
+        """Pick the z-chunk depth that makes MatMult_MFStokes_A11 fastest on the
+        device vector X (CUDA events); leaves it set.  Returns (lz, {lz: ms})."""
+        import torch
+        Y = torch.empty_like(X)
+        st = getattr(self, "stream", None)
+        st = st if hasattr(st, "record_event") else torch.cuda.current_stream()
+        times = {}
+        for lz in candidates:
+            self.set_tiling(lz)
+            if lz == 0:
+                lz = self.tiling
+            if lz in times:
+                continue
+            self.MatMult_MFStokes_A11(X, Y)
+            torch.cuda.synchronize()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(st)
+            for _ in range(reps):
+                self.MatMult_MFStokes_A11(X, Y)
+            b.record(st)
+            b.synchronize()
+            times[lz] = a.elapsed_time(b) / reps
+        best = min(times, key=times.get)
+        self.set_tiling(best)
+        return best, times
+
     def launch_count(self) -> int:
         return int(self._lib.pt_op_launch_count(self._h))
 

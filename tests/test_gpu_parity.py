@@ -161,3 +161,27 @@ def test_large_mesh_properties(torch_cuda, ora):
         assert abs(lhs - rhs) <= 1e-12 * (abs(lhs) + abs(rhs))
         # direct comparison with the oracle at this size
         assert relerr(Au.cpu().numpy(), ora.a11(m.dims, m.coords, eta, u)) < TOL64
+
+
+def test_tiling_schedules_agree_with_the_oracle(ora):
+    """Every z-chunk depth gives the oracle's result to 1e-12 (schedules only
+    reorder the node sums), and set_tiling(0) restores the default."""
+    import torch
+
+    from pt_b200 import MatStokesMF
+    m, eta, mask = M.problem("box:40,9,13", seed=21)
+    x = M.uniform_vec(m.nvel, 22)
+    ref = ora.matmult_a11(m.dims, m.coords, eta, mask, x)
+    with MatStokesMF(*m.dims) as op:
+        op.SetUp(m.coords, eta, mask)
+        default = op.tiling
+        xd = torch.from_numpy(x).cuda()
+        for lz in (1, 2, 3, 5, 13, 40):
+            op.set_tiling(lz)
+            assert op.tiling == min(lz, m.mz)
+            y = op.MatMult_MFStokes_A11(xd).cpu().numpy()
+            assert relerr(y, ref) < 1e-12, lz
+        op.set_tiling(0)
+        assert op.tiling == default
+        best, table = op.autotune_tiling(xd, candidates=(0, 2, 4))
+        assert op.tiling == best and best in table
