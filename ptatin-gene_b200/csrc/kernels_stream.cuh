@@ -47,6 +47,7 @@ struct StreamGrid {
   int LZ, nzc;        // layers per z-chunk, z-chunks
   int px, py, pz;     // colour of this launch
   int nxc, nyc, nzcc; // tiles of this colour per axis
+  int zc0;            // first z-chunk of this launch (parity pz; pz for a whole-box launch)
   int64_t MXP;        // padded row length of the K array (elements)
 };
 
@@ -358,7 +359,7 @@ __global__ void __launch_bounds__(TX, stream_min_blocks<T, TX>()) a11_stream_ker
   // tile of this CTA within the colour class
   const int bid = blockIdx.x;
   const int ixc = bid % g.nxc, iyc = (bid / g.nxc) % g.nyc, izc = bid / (g.nxc * g.nyc);
-  stream_tile<T, TX, MASKED>(g, g.px + 2 * ixc, g.py + 2 * iyc, g.pz + 2 * izc, K, u, mask, y);
+  stream_tile<T, TX, MASKED>(g, g.px + 2 * ixc, g.py + 2 * iyc, g.zc0 + 2 * izc, K, u, mask, y);
 }
 
 // ---------------------------------------------------------------------------
@@ -388,6 +389,7 @@ __global__ void __launch_bounds__(TX, stream_min_blocks<T, TX>()) a11_stream_bat
   g.TX = TX; g.ntx = p.ntx; g.LZ = p.LZ; g.nzc = p.nzc; g.MXP = p.MXP;
   g.px = px; g.py = py; g.pz = pz;
   g.nxc = g.nyc = g.nzcc = 0;
+  g.zc0 = pz;
   stream_tile<T, TX, MASKED>(g, it.y, it.z, it.w, reinterpret_cast<const T *>(p.K), uptr[it.x],
                              MASKED ? p.mask : nullptr, yptr[it.x]);
 }

@@ -225,7 +225,7 @@ __global__ void __launch_bounds__(TM_TX, 2) a11_tmem_kernel(StreamGrid g, const 
 
   const int bid = blockIdx.x;
   const int ixc = bid % g.nxc, iyc = (bid / g.nxc) % g.nyc, izc = bid / (g.nxc * g.nyc);
-  const int tx = g.px + 2 * ixc, ej = g.py + 2 * iyc, zc = g.pz + 2 * izc;
+  const int tx = g.px + 2 * ixc, ej = g.py + 2 * iyc, zc = g.zc0 + 2 * izc;
   const int ex0 = tx * TM_TX;
   const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
   const int ex = ex0 + t;

@@ -16,6 +16,8 @@
 #include <new>
 #include <string>
 #include <type_traits>
+#include <utility>
+#include <vector>
 
 #include "pt_b200.h"
 #include "kernels_colour.cuh"
@@ -81,6 +83,10 @@ struct pt_op {
   uint64_t state;  // bumped whenever coordinates, viscosity or the mask change
   int device;
   cudaMemPool_t pool;  // non-null: buffers are stream-ordered allocations from this pool on `stream`
+  // pipelined host applies: copy streams and per-group events (created on first use)
+  cudaStream_t h2d, d2h;
+  cudaEvent_t ev_in[16], ev_done[16];
+  bool pipe_ready;
 };
 
 namespace {
@@ -171,9 +177,15 @@ pt_status upload_diag_tables()
 
 // ---- streaming kernel: geometry set-up and launch -----------------------------
 
+// Launches the streaming kernel's colour passes over z-chunks [zb, ze)
+// (ze < 0: all).  A sub-range must start at chunk 0 or at an odd chunk and end
+// after an even one, or at the last chunk, so the node sums keep the order of
+// the whole-box launch (the even chunk of a boundary plane stores, the odd one
+// adds).
 template <typename T, int TX, bool MASKED>
-pt_status launch_stream_tx(pt_op *op, const T *K, const T *u, T *y)
+pt_status launch_stream_tx(pt_op *op, const T *K, const T *u, T *y, int zb = 0, int ze = -1)
 {
+  if (ze < 0) ze = op->nzc;
   constexpr size_t smem = ptk::stream_smem_bytes<T, TX>();
   static bool attr_set[64] = {false};
   if (op->device < 64 && !attr_set[op->device]) {
@@ -192,7 +204,8 @@ pt_status launch_stream_tx(pt_op *op, const T *K, const T *u, T *y)
         g.px = px; g.py = py; g.pz = pz;
         g.nxc = (op->ntx - px + 1) / 2;
         g.nyc = (op->my - py + 1) / 2;
-        g.nzcc = (op->nzc - pz + 1) / 2;
+        g.zc0 = zb + ((zb & 1) != pz);  // first chunk >= zb of parity pz
+        g.nzcc = g.zc0 < ze ? (ze - g.zc0 + 1) / 2 : 0;
         const int64_t n = (int64_t)g.nxc * g.nyc * g.nzcc;
         if (n == 0) continue;
         ptk::a11_stream_kernel<T, TX, MASKED><<<(unsigned)n, TX, smem, op->stream>>>(g, K, u, MASKED ? op->d_mask : nullptr, y);
@@ -220,6 +233,7 @@ pt_status launch_tmem(pt_op *op, const double *K, const double *u, double *y)
         g.nxc = (op->ntx - px + 1) / 2;
         g.nyc = (op->my - py + 1) / 2;
         g.nzcc = (op->nzc - pz + 1) / 2;
+        g.zc0 = pz;
         const int64_t n = (int64_t)g.nxc * g.nyc * g.nzcc;
         if (n == 0) continue;
         ptk::a11_tmem_kernel<MASKED><<<(unsigned)n, 128, smem, op->stream>>>(g, K, u, MASKED ? op->d_mask : nullptr, y);
@@ -406,6 +420,87 @@ pt_status host_call(pt_op *op, const double *in, int64_t nin, double *din, doubl
   return PT_OK;
 }
 
+bool is_pinned(const void *p)
+{
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeHost;
+}
+
+// Host-array A11 apply with the copies overlapped with the compute: the box
+// is cut into groups of z-chunks; group g's input node planes go up on one
+// copy stream, its colour passes run when they have arrived, and every node
+// plane that no later group touches comes down on a second copy stream.  The
+// passes are those of the whole-box launch cut by z-range (see
+// launch_stream_tx), so the result is bitwise the one-shot apply's.  Used for
+// pinned host arrays on a one-rank box with the streaming kernel; returns
+// false when that does not apply.
+template <bool MASKED>
+pt_status a11_host_pipelined(pt_op *op, const double *hu, double *hy, bool *done)
+{
+  *done = false;
+  if (!op->full_box || op->a11_kernel != A11_STREAM || !is_pinned(hu) || !is_pinned(hy)) return PT_OK;
+  pt_status s = ensure_geometry(op);
+  if (s != PT_OK) return s;
+  if (!op->geom_ok || op->nzc < 2) return PT_OK;
+  if (!op->pipe_ready) {
+    PT_CUDA(cudaStreamCreateWithFlags(&op->h2d, cudaStreamNonBlocking));
+    PT_CUDA(cudaStreamCreateWithFlags(&op->d2h, cudaStreamNonBlocking));
+    for (int g = 0; g < 16; g++) {
+      PT_CUDA(cudaEventCreateWithFlags(&op->ev_in[g], cudaEventDisableTiming));
+      PT_CUDA(cudaEventCreateWithFlags(&op->ev_done[g], cudaEventDisableTiming));
+    }
+    op->pipe_ready = true;
+  }
+  if (!op->d_u || !op->d_y) return PT_OK;  // callers stage first
+  // groups of chunks [c0, c1]: each ends at an even chunk or at the last one,
+  // so each later group starts at an odd chunk
+  std::vector<std::pair<int, int>> groups;
+  const int per = std::max(1, (op->nzc + 15) / 16);
+  for (int c0 = 0; c0 < op->nzc;) {
+    int c1 = std::min(op->nzc - 1, c0 + per - 1);
+    if (c1 < op->nzc - 1 && (c1 & 1)) c1++;
+    groups.push_back({c0, c1});
+    c0 = c1 + 1;
+  }
+  if ((int)groups.size() > 16) return PT_OK;
+  const int64_t plane = 3 * op->box.XY;  // doubles per node plane
+  const int64_t nplanes = 2 * (int64_t)op->mz + 1;
+  int64_t up = 0, down = 0;  // next plane to upload / download
+  PT_CUDA(cudaEventRecord(op->ev_done[0], op->stream));  // earlier work on the op's stream precedes the copies
+  PT_CUDA(cudaStreamWaitEvent(op->h2d, op->ev_done[0], 0));
+  for (size_t gi = 0; gi < groups.size(); gi++) {
+    const int c0 = groups[gi].first, c1 = groups[gi].second;
+    const bool last = gi + 1 == groups.size();
+    const int64_t top = 2 * (int64_t)std::min((c1 + 1) * op->LZ, op->mz);  // top node plane of the group
+    if (top + 1 > up) {
+      PT_CUDA(cudaMemcpyAsync(op->d_u + up * plane, hu + up * plane, sizeof(double) * (top + 1 - up) * plane,
+                              cudaMemcpyHostToDevice, op->h2d));
+      up = top + 1;
+    }
+    PT_CUDA(cudaEventRecord(op->ev_in[gi], op->h2d));
+    PT_CUDA(cudaStreamWaitEvent(op->stream, op->ev_in[gi], 0));
+    if (op->TX == 32) s = launch_stream_tx<double, 32, MASKED>(op, op->d_K, op->d_u, op->d_y, c0, c1 + 1);
+    else if (op->TX == 64) s = launch_stream_tx<double, 64, MASKED>(op, op->d_K, op->d_u, op->d_y, c0, c1 + 1);
+    else s = launch_stream_tx<double, 128, MASKED>(op, op->d_K, op->d_u, op->d_y, c0, c1 + 1);
+    if (s != PT_OK) return s;
+    PT_CUDA(cudaEventRecord(op->ev_done[gi], op->stream));
+    const int64_t fin = last ? nplanes : top;  // planes below `fin` are final
+    if (fin > down) {
+      PT_CUDA(cudaStreamWaitEvent(op->d2h, op->ev_done[gi], 0));
+      PT_CUDA(cudaMemcpyAsync(hy + down * plane, op->d_y + down * plane, sizeof(double) * (fin - down) * plane,
+                              cudaMemcpyDeviceToHost, op->d2h));
+      down = fin;
+    }
+  }
+  PT_CUDA(cudaStreamSynchronize(op->d2h));
+  *done = true;
+  return PT_OK;
+}
+
 }  // namespace
 
 // ============================================================================
@@ -485,6 +580,16 @@ pt_status pt_op_destroy(pt_op *op)
                   op->d_y, op->d_p, op->d_K, op->d_K32, op->d_bad};
   for (void *b : bufs) op_free(op, b);
   if (op->own_stream && op->stream) cudaStreamDestroy(op->stream);
+  if (op->pipe_ready) {
+    cudaStreamSynchronize(op->h2d);
+    cudaStreamSynchronize(op->d2h);
+    cudaStreamDestroy(op->h2d);
+    cudaStreamDestroy(op->d2h);
+    for (int g = 0; g < 16; g++) {
+      cudaEventDestroy(op->ev_in[g]);
+      cudaEventDestroy(op->ev_done[g]);
+    }
+  }
   free(op);
   return PT_OK;
 }
@@ -615,6 +720,9 @@ pt_status pt_a11_apply_h(pt_op *op, const double *u, double *y)
   pt_status s = check_ready(op, true);
   if (s != PT_OK) return s;
   if ((s = ensure_staging(op)) != PT_OK) return s;
+  bool done = false;
+  if (u && y && (s = a11_host_pipelined<false>(op, u, y, &done)) != PT_OK) return s;
+  if (done) return PT_OK;
   return host_call(op, u, op->nvel, op->d_u, y, op->nvel, op->d_y,
                    [&]() { return launch_a11<double>(op, op->d_coords, op->d_eta, op->d_u, op->d_y, false); });
 }
@@ -693,6 +801,9 @@ pt_status pt_matmult_a11_h(pt_op *op, const double *x, double *y)
   pt_status s = check_ready(op, true);
   if (s != PT_OK) return s;
   if ((s = ensure_staging(op)) != PT_OK) return s;
+  bool done = false;
+  if (x && y && op->has_mask && (s = a11_host_pipelined<true>(op, x, y, &done)) != PT_OK) return s;
+  if (done) return PT_OK;
   return host_call(op, x, op->nvel, op->d_u, y, op->nvel, op->d_y,
                    [&]() { return pt_matmult_a11_d(op, op->d_u, op->d_y); });
 }
@@ -864,6 +975,7 @@ pt_status noalloc_launch(const ptk::StreamGrid &g0, int my, const double *K, con
         g.nxc = (g.ntx - px + 1) / 2;
         g.nyc = (my - py + 1) / 2;
         g.nzcc = (g.nzc - pz + 1) / 2;
+        g.zc0 = pz;
         const int64_t n = (int64_t)g.nxc * g.nyc * g.nzcc;
         if (n == 0) continue;
         ptk::a11_stream_kernel<double, TX, false><<<(unsigned)n, TX, smem, stream>>>(g, K, u, nullptr, y);

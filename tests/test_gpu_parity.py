@@ -185,3 +185,28 @@ def test_tiling_schedules_agree_with_the_oracle(ora):
         assert op.tiling == default
         best, table = op.autotune_tiling(xd, candidates=(0, 2, 4))
         assert op.tiling == best and best in table
+
+
+@pytest.mark.parametrize("lz", [0, 3])
+def test_pipelined_host_apply_is_bitwise_the_device_apply(lz):
+    """With pinned host arrays the host-pointer applies overlap their copies
+    with the compute group by group; the result is bitwise the device apply's
+    (MatShell and SpMVOp level), and pageable arrays give the same."""
+    import torch
+
+    from pt_b200 import MatStokesMF
+    m, eta, mask = M.problem("box:24,10,30", seed=23)
+    x = M.uniform_vec(m.nvel, 24)
+    with MatStokesMF(*m.dims) as op:
+        op.SetUp(m.coords, eta, mask)
+        op.set_tiling(lz)
+        xd = torch.from_numpy(x).cuda()
+        y_dev = op.MatMult_MFStokes_A11(xd).cpu().numpy()
+        a_dev = op.MFStokesWrapper_A11(xd).cpu().numpy()
+        xp = torch.from_numpy(x).pin_memory()
+        yp = torch.empty(m.nvel, dtype=torch.float64).pin_memory()
+        op.MatMult_MFStokes_A11(xp.numpy(), yp.numpy())
+        assert np.array_equal(yp.numpy(), y_dev)
+        op.MFStokesWrapper_A11(xp.numpy(), yp.numpy())
+        assert np.array_equal(yp.numpy(), a_dev)
+        assert np.array_equal(op.MatMult_MFStokes_A11(x.copy()), y_dev)
