@@ -163,36 +163,64 @@ def barrier(pg, device):
     torch.cuda.synchronize()
 
 
-def cpu_reference_sample(workload_slab=("c2", 16), seconds=12.0, kind="avx"):
-    """Time the reference's own A11 (oracle/_ref) on a z-slab of the workload."""
+def reference_sample_problem(workload):
+    """The CPU sample of a workload: the whole problem when it has at most
+    300k elements, else a 16-layer z-slab of it (same generators)."""
+    from pt_b200 import mesh as M
+    m, eta, mask = M.problem(workload, seed=0) if workload != "c2" else (None, None, None)
+    if m is not None and m.nel <= 300_000:
+        return m, eta, mask, f"the whole {m.mx}x{m.my}x{m.mz} problem"
+    if m is None or workload == "c2":
+        m = M.make_mesh(128, 128, 16, perturb=0.05, seed=0)
+        eta = M.eta_layered(m, seed=1)
+        return m, eta, M.bc_mask_freeslip(*m.dims), "a 128x128x16 slab of the 128^3 workload"
+    mx, my, mz = m.dims
+    ms = M.make_mesh(mx, my, 16, perturb=0.05, seed=0)
+    from pt_b200.mesh import eta_loguniform_qp
+    return ms, eta_loguniform_qp(ms, seed=1), M.bc_mask_freeslip(*ms.dims), f"a {mx}x{my}x16 slab"
+
+
+def cpu_reference_sample(workload="c2", seconds=12.0, kind="avx", ops=False):
+    """Time the reference's own A11 (oracle/_ref, all host cores) on the
+    workload's CPU sample; with ops=True also its diag, B and B^T."""
     import oracle
     from pt_b200 import mesh as M
     if not oracle.RefCPU.available():
         oracle.build()
     r = oracle.RefCPU()
-    mz = workload_slab[1]
-    m = M.make_mesh(128, 128, mz, perturb=0.05, seed=0)
-    eta = M.eta_layered(m, seed=1)
-    mask = M.bc_mask_freeslip(*m.dims)
+    m, eta, mask, what = reference_sample_problem(workload)
     x = M.uniform_vec(m.nvel, 7)
     x[mask.astype(bool)] = 0.0
-    r.a11(m.dims, m.coords, eta, x, kind)  # warm-up
-    times = []
-    t_end = time.perf_counter() + seconds
-    while time.perf_counter() < t_end or len(times) < 2:
-        t0 = time.perf_counter()
-        r.a11(m.dims, m.coords, eta, x, kind)
-        times.append(time.perf_counter() - t0)
-    best = min(times)
-    return {
+    p = M.uniform_vec(m.npres, 8)
+
+    def best_of(fn, budget):
+        fn()  # warm-up
+        times, t_end = [], time.perf_counter() + budget
+        while time.perf_counter() < t_end or len(times) < 2:
+            t0 = time.perf_counter()
+            fn()
+            times.append(time.perf_counter() - t0)
+        return min(times), len(times)
+
+    best, nrep = best_of(lambda: r.a11(m.dims, m.coords, eta, x, kind), seconds)
+    out = {
         "value": m.nvel / best / 1e9,
         "unit": UNIT,
         "cores": os.cpu_count(),
         "kind": "reference",
-        "sample": f"reference {kind} A11 (MFStokesWrapper_A11_AVX, OpenMP {os.cpu_count()} threads) on a "
-                  f"128x128x{mz} slab of the 128^3 workload, best of {len(times)} applies",
+        "sample": f"reference {kind} A11 (MFStokesWrapper_A11_AVX, OpenMP {os.cpu_count()} threads) on "
+                  f"{what}, best of {nrep} applies",
         "seconds_per_apply": best,
     }
+    if ops:
+        budget = max(1.0, seconds / 4)
+        out["ops_seconds"] = {
+            "diag": best_of(lambda: r.diag(m.dims, m.coords, eta), budget)[0],
+            "a21": best_of(lambda: r.a21(m.dims, m.coords, x), budget)[0],
+            "a12": best_of(lambda: r.a12(m.dims, m.coords, p, "avx"), budget)[0],
+        }
+        out["ops_gdofs"] = {k: m.nvel / v / 1e9 for k, v in out["ops_seconds"].items()}
+    return out
 
 
 def run_reference(args):
@@ -209,10 +237,7 @@ def run_reference(args):
         return 0
     from pt_b200 import mesh as M
     r = oracle.RefCPU()
-    mz = 16
-    m = M.make_mesh(128, 128, mz, perturb=0.05, seed=0)
-    eta = M.eta_layered(m, seed=1)
-    mask = M.bc_mask_freeslip(*m.dims)
+    m, eta, mask, what = reference_sample_problem(args.workload)
     x = M.uniform_vec(m.nvel, 7)
     x[mask.astype(bool)] = 0.0
     for _ in range(args.warmup):
@@ -226,11 +251,10 @@ def run_reference(args):
         "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": "A11 FP64 apply, 128x128x16 slab of the 128^3 Q2 box (perturbed +-0.05h, layered "
-                               "eta 1e6 contrast), reference CPU (oracle/_ref, avx)",
+        "config": {"workload": f"A11 FP64 apply on {what} ({args.workload}), reference CPU (oracle/_ref, avx)",
                    "global_batch": 1, "seq_len": 0, "parallelism": "cpu-openmp"},
         "cpu_baseline": {"value": v, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
-                         "sample": "128x128x16 slab, MFStokesWrapper_A11_AVX compiled from the reference sources"},
+                         "sample": f"{what}, MFStokesWrapper_A11_AVX compiled from the reference sources"},
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
@@ -270,7 +294,7 @@ def run_ours(args):
 
     # ---- tile schedule by the autotuner (untimed), then the headline --------
     tiling = {"lz": op.tiling, "autotune": None}
-    if not args.no_autotune and args.a11_op in ("b200", "b200_tmem"):
+    if not args.no_autotune and op.a11_op in ("b200_stream", "b200_tmem"):
         best, table = op.autotune_tiling(x)
         tiling = {"lz": best, "autotune_ms": {str(k): round(v, 4) for k, v in table.items()}}
     # ---- headline: FP64 A11 (MatShell level), device resident ----------------
@@ -323,7 +347,7 @@ def run_ours(args):
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         try:
-            cpu = cpu_reference_sample(seconds=args.cpu_seconds)
+            cpu = cpu_reference_sample(args.workload, seconds=args.cpu_seconds, ops=not args.quick)
         except Exception as e:  # pragma: no cover
             cpu = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
                    "sample": f"unavailable: {e}"}

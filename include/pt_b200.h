@@ -310,10 +310,13 @@ pt_status pt_server_timers(const pt_server *server, double *enqueue, double *adm
 /* ---- selection, in the style of -a11_op --------------------------------- */
 
 /* Select the A11 kernel by name, like the reference's -a11_op function list
- * (src/stokes_operators.c:123-154).  Names: "b200" (default, the streaming
- * kernel with precomputed Gauss-point geometry), "b200_tmem" (its variant with
- * TMEM accumulators, FP64 rows of 65..128 elements) and "b200_colour"
- * (8-colour element kernel).  Unknown names give
+ * (src/stokes_operators.c:123-154).  Names: "b200" (default: stored element
+ * matrices for one-rank boxes of at most 4096 elements, the streaming kernel
+ * above), "b200_stream" (the streaming kernel with precomputed Gauss-point
+ * geometry), "b200_ebe" (stored 81x81 element matrices, element GEMV + node
+ * gather; one-rank boxes), "b200_tmem" (the streaming kernel with TMEM
+ * accumulators, FP64 rows of 65..128 elements) and "b200_colour" (8-colour
+ * element kernel).  The getter returns the kernel in use.  Unknown names give
  * PT_ERR_BAD_ARG, as the reference's SETERRQ1 "No -a11_op %s". */
 pt_status pt_op_set_a11_kernel(pt_op *op, const char *name);
 const char *pt_op_get_a11_kernel(const pt_op *op);

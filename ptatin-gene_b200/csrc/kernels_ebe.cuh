@@ -1,0 +1,175 @@
+// Stored element matrices ("b200_ebe" and the small multigrid levels).
+//
+// An element's 81x81 matrix is the colour kernel's element operator applied
+// to the unit vectors (exact FP64 arithmetic of the reference's element
+// kernel, adjugate form), stored column-major per element (Ae[e][j][i], j =
+// 3n+l the input dof) in FP64 or FP32.  An apply is two launches: a GEMV per
+// element into per-element outputs, and a gather per dof that sums the (at
+// most 8) element contributions of its node in a fixed order -- a node-
+// centred scatter, deterministic without atomics.  It reads 52 KB per
+// element (FP64), so it pays only where the streaming kernel is latency-bound
+// (small boxes: a few CTAs, each marching its layers one after another).
+#pragma once
+
+#include <cstdint>
+
+#include "kernels_colour.cuh"
+#include "q2_core.cuh"
+
+namespace ptk {
+
+
+// Column j of element e's matrix: the element operator of the colour kernel
+// applied to the unit vector e_j.  Block = element, 81 threads.
+template <typename T>
+__global__ void __launch_bounds__(96) element_matrix_kernel(Box b, const double *__restrict__ coords,
+                                                            const double *__restrict__ eta, T *__restrict__ Ae)
+{
+  const int j = threadIdx.x;
+  if (j >= 81) return;
+  const int64_t e = blockIdx.x;
+  const int ei = (int)(e % b.mx), ej = (int)((e / b.mx) % b.my), ek = (int)(e / ((int64_t)b.mx * b.my));
+  int64_t nid[27];
+  element_nodes(b, ei, ej, ek, nid);
+  double Jg[3][3][27], Xq[3][27];
+  element_jacobian(coords, nid, Jg, Xq);
+  const int nj = j / 3, lj = j % 3;
+  double Ug[3][3][27];
+  for (int k = 0; k < 3; k++)
+    for (int l = 0; l < 3; l++)
+      for (int q = 0; q < 27; q++) Ug[k][l][q] = 0.0;
+  {
+    double f[27], I[27];
+    for (int n = 0; n < 27; n++) f[n] = n == nj ? 1.0 : 0.0;
+    q2::interp(f, I);
+    q2::grad_colloc(I, Ug[0][lj], Ug[1][lj], Ug[2][lj]);
+  }
+  for (int q = 0; q < 27; q++) {
+    double J[3][3], adj[3][3], G[3][3], d[3][3];
+    for (int k = 0; k < 3; k++)
+      for (int l = 0; l < 3; l++) {
+        J[k][l] = Jg[k][l][q];
+        G[k][l] = Ug[k][l][q];
+      }
+    const double det = q2::adjugate(J, adj);
+    const double c = q2::weight(q) * eta[27 * e + q] / det;
+    q2::qp_viscous(adj, c, G, d);
+    for (int k = 0; k < 3; k++)
+      for (int l = 0; l < 3; l++) Ug[k][l][q] = d[k][l];
+  }
+  T *col = Ae + (e * 81 + j) * 81;
+  for (int l = 0; l < 3; l++) {
+    double r[27], f[27];
+    q2::grad_colloc_t(Ug[0][l], Ug[1][l], Ug[2][l], r);
+    q2::interp_t(r, f);
+    for (int n = 0; n < 27; n++) col[3 * n + l] = (T)f[n];
+  }
+}
+
+// ye[e][i] = sum_j Ae[e][j][i] u_j (MASKED: Dirichlet entries of u taken as 0).
+template <typename T, bool MASKED>
+__global__ void __launch_bounds__(96) ebe_apply_kernel(Box b, const T *__restrict__ Ae, const T *__restrict__ u,
+                                                       const uint8_t *__restrict__ mask, T *__restrict__ ye)
+{
+  __shared__ T ue[81];
+  const int t = threadIdx.x;
+  const int64_t e = blockIdx.x;
+  const int ei = (int)(e % b.mx), ej = (int)((e / b.mx) % b.my), ek = (int)(e / ((int64_t)b.mx * b.my));
+  if (t < 81) {
+    const int n = t / 3, l = t % 3;
+    const int64_t node = b.off + (2 * ei + n % 3) + (2 * (int64_t)ej + (n / 3) % 3) * b.X + (2 * (int64_t)ek + n / 9) * b.XY;
+    const int64_t k = 3 * node + l;
+    ue[t] = (MASKED && mask[k]) ? T(0) : u[k];
+  }
+  __syncthreads();
+  if (t < 81) {
+    const T *A = Ae + e * 6561 + t;
+    T acc = T(0);
+#pragma unroll 9
+    for (int jj = 0; jj < 81; jj++) acc = fma(A[jj * 81], ue[jj], acc);
+    ye[e * 81 + t] = acc;
+  }
+}
+
+// y_k = sum over the (<= 8) elements of node k of their ye entry, in a fixed
+// order (MASKED: y_k = x_k on Dirichlet dofs).  One-rank boxes (node box =
+// element box).
+template <typename T, bool MASKED>
+__global__ void ebe_gather_kernel(Box b, const T *__restrict__ ye, const T *__restrict__ x,
+                                  const uint8_t *__restrict__ mask, T *__restrict__ y)
+{
+  const int64_t n = 3 * b.XY * (2 * (int64_t)b.mz + 1);
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) {
+    if (MASKED && mask[t]) {
+      y[t] = x[t];
+      continue;
+    }
+    const int l = (int)(t % 3);
+    const int64_t node = t / 3;
+    const int i = (int)(node % b.X), j = (int)((node / b.X) % (2 * b.my + 1)), k = (int)(node / b.XY);
+    // per axis: (element, local index) pairs, lower element first
+    int ex[2], lx[2], nx = 0, ey[2], ly[2], ny = 0, ez[2], lz[2], nz = 0;
+    if (i & 1) { ex[0] = i >> 1; lx[0] = 1; nx = 1; }
+    else {
+      if (i > 0) { ex[nx] = (i >> 1) - 1; lx[nx++] = 2; }
+      if ((i >> 1) < b.mx) { ex[nx] = i >> 1; lx[nx++] = 0; }
+    }
+    if (j & 1) { ey[0] = j >> 1; ly[0] = 1; ny = 1; }
+    else {
+      if (j > 0) { ey[ny] = (j >> 1) - 1; ly[ny++] = 2; }
+      if ((j >> 1) < b.my) { ey[ny] = j >> 1; ly[ny++] = 0; }
+    }
+    if (k & 1) { ez[0] = k >> 1; lz[0] = 1; nz = 1; }
+    else {
+      if (k > 0) { ez[nz] = (k >> 1) - 1; lz[nz++] = 2; }
+      if ((k >> 1) < b.mz) { ez[nz] = k >> 1; lz[nz++] = 0; }
+    }
+    T acc = T(0);
+    for (int c = 0; c < nz; c++)
+      for (int bb = 0; bb < ny; bb++)
+        for (int a = 0; a < nx; a++) {
+          const int64_t e = ex[a] + (int64_t)b.mx * (ey[bb] + (int64_t)b.my * ez[c]);
+          acc += ye[e * 81 + 3 * (lx[a] + 3 * ly[bb] + 9 * lz[c]) + l];
+        }
+    y[t] = acc;
+  }
+}
+
+// diag(A11)_k = sum over the elements of node k of their matrix diagonal
+// entry (fixed order, as ebe_gather_kernel).
+__global__ void ebe_diag_kernel(Box b, const double *__restrict__ Ae, double *__restrict__ d)
+{
+  const int64_t n = 3 * b.XY * (2 * (int64_t)b.mz + 1);
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) {
+    const int l = (int)(t % 3);
+    const int64_t node = t / 3;
+    const int i = (int)(node % b.X), j = (int)((node / b.X) % (2 * b.my + 1)), k = (int)(node / b.XY);
+    int ex[2], lx[2], nx = 0, ey[2], ly[2], ny = 0, ez[2], lz[2], nz = 0;
+    if (i & 1) { ex[0] = i >> 1; lx[0] = 1; nx = 1; }
+    else {
+      if (i > 0) { ex[nx] = (i >> 1) - 1; lx[nx++] = 2; }
+      if ((i >> 1) < b.mx) { ex[nx] = i >> 1; lx[nx++] = 0; }
+    }
+    if (j & 1) { ey[0] = j >> 1; ly[0] = 1; ny = 1; }
+    else {
+      if (j > 0) { ey[ny] = (j >> 1) - 1; ly[ny++] = 2; }
+      if ((j >> 1) < b.my) { ey[ny] = j >> 1; ly[ny++] = 0; }
+    }
+    if (k & 1) { ez[0] = k >> 1; lz[0] = 1; nz = 1; }
+    else {
+      if (k > 0) { ez[nz] = (k >> 1) - 1; lz[nz++] = 2; }
+      if ((k >> 1) < b.mz) { ez[nz] = k >> 1; lz[nz++] = 0; }
+    }
+    double acc = 0.0;
+    for (int c = 0; c < nz; c++)
+      for (int bb = 0; bb < ny; bb++)
+        for (int a = 0; a < nx; a++) {
+          const int64_t e = ex[a] + (int64_t)b.mx * (ey[bb] + (int64_t)b.my * ez[c]);
+          const int jj = 3 * (lx[a] + 3 * ly[bb] + 9 * lz[c]) + l;
+          acc += Ae[e * 6561 + (int64_t)jj * 81 + jj];
+        }
+    d[t] = acc;
+  }
+}
+
+}  // namespace ptk

@@ -23,6 +23,7 @@
 #include "kernels_colour.cuh"
 #include "kernels_stream.cuh"
 #include "kernels_tmem.cuh"
+#include "kernels_ebe.cuh"
 
 namespace {
 
@@ -56,7 +57,13 @@ pt_status fail(pt_status s, const char *fmt, ...)
                   __LINE__);                                                                       \
   } while (0)
 
-enum A11Kernel { A11_STREAM = 0, A11_COLOUR = 1, A11_TMEM = 2 };
+enum A11Kernel { A11_STREAM = 0, A11_COLOUR = 1, A11_TMEM = 2, A11_EBE = 3 };
+
+// "b200" picks stored element matrices for one-rank boxes up to this many
+// elements (FP64 + FP32 matrices: 78 KB per element) and the streaming kernel
+// above.  Measured at 8^3: 2 launches vs a 0.2 ms latency chain of 4 colour
+// launches.
+constexpr int64_t EBE_AUTO_MAX_ELEMENTS = 4096;
 
 }  // namespace
 
@@ -77,12 +84,16 @@ struct pt_op {
   unsigned int *d_bad;
   int64_t MXP;
   int TX, ntx, LZ, nzc;
-  bool geom_dirty, geom_ok, full_box;
+  bool geom_dirty, geom_ok, full_box, ebe_valid;
   int a11_kernel;
   int64_t launches;
   uint64_t state;  // bumped whenever coordinates, viscosity or the mask change
   int device;
   cudaMemPool_t pool;  // non-null: buffers are stream-ordered allocations from this pool on `stream`
+  // stored element matrices (A11_EBE): FP64 and FP32, per-element outputs
+  double *d_Ae;
+  float *d_Ae32;
+  double *d_ye;
   // pipelined host applies: copy streams and per-group events (created on first use)
   cudaStream_t h2d, d2h;
   cudaEvent_t ev_in[16], ev_done[16];
@@ -288,6 +299,53 @@ pt_status ensure_geometry(pt_op *op)
   PT_CUDA(cudaStreamSynchronize(op->stream));
   op->geom_ok = (bad == 0);
   op->geom_dirty = false;
+  op->ebe_valid = false;
+  return PT_OK;
+}
+
+// Element matrices of the current geometry (A11_EBE), built on first use.
+pt_status ensure_ebe(pt_op *op)
+{
+  if (op->ebe_valid) return PT_OK;
+  if (!op->d_Ae) {
+    PT_CUDA(op_alloc(op, (void **)&op->d_Ae, sizeof(double) * 6561 * op->nel));
+    PT_CUDA(op_alloc(op, (void **)&op->d_Ae32, sizeof(float) * 6561 * op->nel));
+    PT_CUDA(op_alloc(op, (void **)&op->d_ye, sizeof(double) * 81 * op->nel));
+  }
+  ptk::element_matrix_kernel<double><<<(unsigned)op->nel, 96, 0, op->stream>>>(op->box, op->d_coords, op->d_eta,
+                                                                               op->d_Ae);
+  PT_LAUNCHED(op);
+  ptk::element_matrix_kernel<float><<<(unsigned)op->nel, 96, 0, op->stream>>>(op->box, op->d_coords, op->d_eta,
+                                                                              op->d_Ae32);
+  PT_LAUNCHED(op);
+  op->ebe_valid = true;
+  return PT_OK;
+}
+
+template <typename T>
+const T *op_Ae(const pt_op *op);
+template <>
+const double *op_Ae<double>(const pt_op *op) { return op->d_Ae; }
+template <>
+const float *op_Ae<float>(const pt_op *op) { return op->d_Ae32; }
+
+template <typename T>
+pt_status launch_ebe(pt_op *op, const T *u, T *y, bool masked)
+{
+  pt_status s = ensure_ebe(op);
+  if (s != PT_OK) return s;
+  T *ye = reinterpret_cast<T *>(op->d_ye);
+  if (masked) {
+    ptk::ebe_apply_kernel<T, true><<<(unsigned)op->nel, 96, 0, op->stream>>>(op->box, op_Ae<T>(op), u, op->d_mask, ye);
+    PT_LAUNCHED(op);
+    ptk::ebe_gather_kernel<T, true><<<grid_stride_blocks(op->nvel), 256, 0, op->stream>>>(op->box, ye, u, op->d_mask,
+                                                                                         y);
+  } else {
+    ptk::ebe_apply_kernel<T, false><<<(unsigned)op->nel, 96, 0, op->stream>>>(op->box, op_Ae<T>(op), u, nullptr, ye);
+    PT_LAUNCHED(op);
+    ptk::ebe_gather_kernel<T, false><<<grid_stride_blocks(op->nvel), 256, 0, op->stream>>>(op->box, ye, u, nullptr, y);
+  }
+  PT_LAUNCHED(op);
   return PT_OK;
 }
 
@@ -297,7 +355,9 @@ pt_status ensure_geometry(pt_op *op)
 // launch_a11 does it for ghost nodes), so MatMult needs no separate pass.
 bool a11_sets_bc_rows(const pt_op *op)
 {
-  return (op->a11_kernel == A11_STREAM || op->a11_kernel == A11_TMEM) && op->geom_ok && !op->geom_dirty;
+  const bool stream = op->a11_kernel == A11_STREAM || op->a11_kernel == A11_TMEM;
+  const bool ebe = op->a11_kernel == A11_EBE && op->full_box;
+  return (stream || ebe) && op->geom_ok && !op->geom_dirty;
 }
 
 template <typename T>
@@ -310,6 +370,11 @@ const float *op_K<float>(const pt_op *op) { return op->d_K32; }
 template <typename T>
 pt_status launch_a11(pt_op *op, const T *coords, const T *eta, const T *u, T *y, bool masked)
 {
+  if (op->a11_kernel == A11_EBE && op->full_box) {
+    pt_status s = ensure_geometry(op);
+    if (s != PT_OK) return s;
+    if (op->geom_ok) return launch_ebe<T>(op, u, y, masked);
+  }
   if (op->a11_kernel == A11_STREAM || op->a11_kernel == A11_TMEM) {
     pt_status s = ensure_geometry(op);
     if (s != PT_OK) return s;
@@ -344,7 +409,18 @@ pt_status launch_a11(pt_op *op, const T *coords, const T *eta, const T *u, T *y,
 
 pt_status diag_d(pt_op *op, double *d)
 {
-  pt_status s = upload_diag_tables();
+  pt_status s;
+  if (op->a11_kernel == A11_EBE && op->full_box) {
+    // the stored element matrices carry the diagonal: one gather
+    if ((s = ensure_geometry(op)) != PT_OK) return s;
+    if (op->geom_ok) {
+      if ((s = ensure_ebe(op)) != PT_OK) return s;
+      ptk::ebe_diag_kernel<<<grid_stride_blocks(op->nvel), 256, 0, op->stream>>>(op->box, op->d_Ae, d);
+      PT_LAUNCHED(op);
+      return PT_OK;
+    }
+  }
+  s = upload_diag_tables();
   if (s != PT_OK) return s;
   PT_CUDA(cudaMemsetAsync(d, 0, sizeof(double) * op->nvel, op->stream));
   for (int c = 0; c < 8; c++) {
@@ -459,7 +535,7 @@ pt_status a11_host_pipelined(pt_op *op, const double *hu, double *hy, bool *done
   // groups of chunks [c0, c1]: each ends at an even chunk or at the last one,
   // so each later group starts at an odd chunk
   std::vector<std::pair<int, int>> groups;
-  const int per = std::max(1, (op->nzc + 15) / 16);
+  const int per = std::max(1, (op->nzc + 7) / 8);
   for (int c0 = 0; c0 < op->nzc;) {
     int c1 = std::min(op->nzc - 1, c0 + per - 1);
     if (c1 < op->nzc - 1 && (c1 & 1)) c1++;
@@ -536,13 +612,13 @@ static pt_status op_create_impl(const pt_mesh_desc *desc, cudaMemPool_t pool, cu
   op->nvel = 3 * nnodes;
   op->nel = (int64_t)desc->mx * desc->my * desc->mz;
   op->npres = 4 * op->nel;
-  op->a11_kernel = A11_STREAM;
+  op->full_box = (nx == 2 * (int64_t)desc->mx + 1) && (ny == 2 * (int64_t)desc->my + 1) &&
+                 (nz == 2 * (int64_t)desc->mz + 1);
+  op->a11_kernel = (op->full_box && op->nel <= EBE_AUTO_MAX_ELEMENTS) ? A11_EBE : A11_STREAM;
   op->TX = desc->mx <= 32 ? 32 : (desc->mx <= 64 ? 64 : 128);
   op->ntx = (desc->mx + op->TX - 1) / op->TX;
   op->MXP = (int64_t)op->ntx * op->TX;
   pt_op_set_tiling(op, 0);
-  op->full_box = (nx == 2 * (int64_t)desc->mx + 1) && (ny == 2 * (int64_t)desc->my + 1) &&
-                 (nz == 2 * (int64_t)desc->mz + 1);
   op->geom_dirty = true;
   cudaError_t e = cudaGetDevice(&op->device);
   if (pool) {
@@ -577,7 +653,7 @@ pt_status pt_op_destroy(pt_op *op)
   // pooled ops free in stream order (after the op's queued work); others wait
   if (op->stream && !op->pool) cudaStreamSynchronize(op->stream);
   void *bufs[] = {op->d_coords, op->d_eta, op->d_coords32, op->d_eta32, op->d_mask, op->d_u,
-                  op->d_y, op->d_p, op->d_K, op->d_K32, op->d_bad};
+                  op->d_y, op->d_p, op->d_K, op->d_K32, op->d_bad, op->d_Ae, op->d_Ae32, op->d_ye};
   for (void *b : bufs) op_free(op, b);
   if (op->own_stream && op->stream) cudaStreamDestroy(op->stream);
   if (op->pipe_ready) {
@@ -868,7 +944,9 @@ pt_status pt_matmult_a21_h(pt_op *op, const double *u, double *yp)
 pt_status pt_op_set_a11_kernel(pt_op *op, const char *name)
 {
   if (!op || !name) return fail(PT_ERR_BAD_ARG, "NULL argument");
-  if (!strcmp(name, "b200")) op->a11_kernel = A11_STREAM;
+  if (!strcmp(name, "b200")) op->a11_kernel = (op->full_box && op->nel <= EBE_AUTO_MAX_ELEMENTS) ? A11_EBE : A11_STREAM;
+  else if (!strcmp(name, "b200_stream")) op->a11_kernel = A11_STREAM;
+  else if (!strcmp(name, "b200_ebe")) op->a11_kernel = A11_EBE;
   else if (!strcmp(name, "b200_colour")) op->a11_kernel = A11_COLOUR;
   else if (!strcmp(name, "b200_tmem")) op->a11_kernel = A11_TMEM;
   else return fail(PT_ERR_BAD_ARG, "No -a11_op %s", name);
@@ -896,7 +974,12 @@ int32_t pt_op_get_tiling(const pt_op *op) { return op ? op->LZ : 0; }
 const char *pt_op_get_a11_kernel(const pt_op *op)
 {
   if (!op) return "";
-  return op->a11_kernel == A11_STREAM ? "b200" : (op->a11_kernel == A11_TMEM ? "b200_tmem" : "b200_colour");
+  switch (op->a11_kernel) {
+    case A11_STREAM: return "b200_stream";
+    case A11_TMEM: return "b200_tmem";
+    case A11_EBE: return "b200_ebe";
+    default: return "b200_colour";
+  }
 }
 
 int64_t pt_op_launch_count(const pt_op *op) { return op ? op->launches : 0; }

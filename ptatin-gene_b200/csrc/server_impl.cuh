@@ -551,6 +551,7 @@ pt_status srv_admit(pt_server *s, SrvReq *r, int slot)
   if (e != PT_OK) return e;
   pt_op *op = r->op;
   if (!op->full_box) return fail(PT_ERR_UNSUPPORTED, "request %lld: one-rank boxes only", (long long)r->id);
+  op->a11_kernel = A11_STREAM;  // the batch runs the streaming kernel; set-up applies use the same
   if (s->o.lz > 0) {
     op->LZ = std::min(s->o.lz, op->mz);
     op->nzc = (op->mz + op->LZ - 1) / op->LZ;

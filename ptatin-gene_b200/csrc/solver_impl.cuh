@@ -378,7 +378,8 @@ pt_status mg_coarsen(const pt_op *f, const double *vf_f, double *vf_c, pt_op **o
   if (st != PT_OK) return st;
   *out = c;  // the caller owns it from here on
   if ((st = pt_op_set_stream(c, (void *)f->stream)) != PT_OK) return st;
-  c->a11_kernel = f->a11_kernel;
+  // small levels keep their own element matrices (mg_level_setup)
+  c->a11_kernel = (f->a11_kernel == A11_EBE) ? A11_STREAM : f->a11_kernel;
   const MgBox fb = mgbox(f), cb = mgbox(c);
   inject_coords_kernel<<<vgrid(c->nnodes), 256, 0, c->stream>>>(fb, cb, f->d_coords, c->d_coords);
   PT_LAUNCHED(c);
@@ -407,7 +408,7 @@ pt_status mg_dense_inverse(pt_mg_level &L, bool fp32)
   const int64_t n = L.n, nel = op->nel;
   double *dAe = nullptr;
   PT_CUDA(cudaMalloc(&dAe, sizeof(double) * 6561 * nel));
-  element_matrix_kernel<double><<<(unsigned)nel, 96, 0, op->stream>>>(op->box, op->d_coords, op->d_eta, dAe);
+  ptk::element_matrix_kernel<double><<<(unsigned)nel, 96, 0, op->stream>>>(op->box, op->d_coords, op->d_eta, dAe);
   std::vector<double> Ae(6561 * nel), A(n * n, 0.0);
   std::vector<uint8_t> mask(n);
   cudaError_t e = cudaGetLastError();
@@ -500,10 +501,10 @@ pt_status mg_level_setup(pt_solver *s, pt_mg &mg, pt_mg_level &L, const pt_op *n
     PT_CUDA(cudaMalloc(&L.Ae, ts * 6561 * L.nel));
     PT_CUDA(cudaMalloc(&L.ye, ts * 81 * L.nel));
     if (mg.fp32)
-      element_matrix_kernel<float><<<(unsigned)L.nel, 96, 0, L.op->stream>>>(L.op->box, L.op->d_coords, L.op->d_eta,
+      ptk::element_matrix_kernel<float><<<(unsigned)L.nel, 96, 0, L.op->stream>>>(L.op->box, L.op->d_coords, L.op->d_eta,
                                                                              (float *)L.Ae);
     else
-      element_matrix_kernel<double><<<(unsigned)L.nel, 96, 0, L.op->stream>>>(L.op->box, L.op->d_coords,
+      ptk::element_matrix_kernel<double><<<(unsigned)L.nel, 96, 0, L.op->stream>>>(L.op->box, L.op->d_coords,
                                                                               L.op->d_eta, (double *)L.Ae);
     PT_LAUNCHED(L.op);
   }

@@ -29,7 +29,7 @@ try:  # torch is plumbing only (device memory, streams); optional on CPU hosts
 except Exception:  # pragma: no cover
     torch = None
 
-A11_OPS = ("b200", "b200_tmem", "b200_colour")
+A11_OPS = ("b200", "b200_stream", "b200_ebe", "b200_tmem", "b200_colour")
 
 
 def _is_dev(a) -> bool:

@@ -21,7 +21,7 @@ def problems():
     for i, (mx, my, mz) in enumerate(SHAPES):
         m = M.make_mesh(mx, my, mz, perturb=0.05, seed=i)
         eta = M.eta_per_element(m, contrast=10.0 ** (2 + 2 * (i % 3)), seed=i)
-        op = MatStokesMF(mx, my, mz)
+        op = MatStokesMF(mx, my, mz, a11_op="b200_stream")
         op.SetUp(m.coords, eta, M.bc_mask_freeslip(mx, my, mz))
         ops.append(op)
         us.append(torch.from_numpy(M.uniform_vec(m.nvel, 50 + i)).cuda())

@@ -32,7 +32,7 @@ def make_op(m, eta=None, mask=None, a11_op="b200"):
     return op
 
 
-@pytest.mark.parametrize("a11_op", ["b200", "b200_colour"])
+@pytest.mark.parametrize("a11_op", ["b200_stream", "b200_ebe", "b200_colour"])
 @pytest.mark.parametrize("name", golden_names())
 def test_spmvop_level_matches_reference(torch_cuda, name, a11_op):
     g = load_golden(name)
@@ -52,11 +52,12 @@ def test_spmvop_level_matches_reference(torch_cuda, name, a11_op):
 @pytest.mark.parametrize("workload", ["c0", "box:3,2,4", "box:1,1,1", "box:1,2,3", "box:7,5,3", "box:33,2,2",
                                       "box:2,40,1", "box:64,3,1", "box:130,2,3", "box:257,1,2", "box:3,2,40",
                                       "box:65,9,7", "box:128,3,5", "box:100,4,11"])
-def test_matshell_level_matches_oracle(torch_cuda, ora, workload):
+@pytest.mark.parametrize("a11_op", ["b200", "b200_stream"])
+def test_matshell_level_matches_oracle(torch_cuda, ora, workload, a11_op):
     m, eta, mask = M.problem(workload, seed=5)
     x = M.uniform_vec(m.nvel, 6)
     p = M.uniform_vec(m.npres, 7)
-    with make_op(m, eta, mask) as op:
+    with make_op(m, eta, mask, a11_op) as op:
         assert relerr(op.MatMult_MFStokes_A11(x), ora.matmult_a11(m.dims, m.coords, eta, mask, x)) < TOL64
         assert relerr(op.MatGetDiagonal_MFStokes_A11(), ora.getdiag_a11(m.dims, m.coords, eta, mask)) < TOL64
         assert relerr(op.MatMult_MFStokes_A12(p), ora.matmult_a12(m.dims, m.coords, mask, p)) < TOL64
@@ -91,15 +92,16 @@ def test_apply_is_deterministic(torch_cuda):
         assert torch.equal(y1, y2)
 
 
-@pytest.mark.parametrize("other", ["b200_colour", "b200_tmem"])
+@pytest.mark.parametrize("other", ["b200_colour", "b200_tmem", "b200_ebe"])
 @pytest.mark.parametrize("workload", ["box:40,7,5", "box:150,3,9", "box:128,4,6"])
 def test_kernels_agree(torch_cuda, workload, other):
-    """The default streaming kernel, its TMEM-accumulator variant (rows of
-    65..128 elements) and the 8-colour kernel agree to FP64 rounding."""
+    """The streaming kernel, its TMEM-accumulator variant (rows of 65..128
+    elements), the stored element matrices and the 8-colour kernel agree to
+    FP64 rounding."""
     torch = torch_cuda
     m, eta, mask = M.problem(workload, seed=8)
     xd = torch.from_numpy(M.uniform_vec(m.nvel, 9)).cuda()
-    with make_op(m, eta, mask, "b200") as a, make_op(m, eta, mask, other) as b:
+    with make_op(m, eta, mask, "b200_stream") as a, make_op(m, eta, mask, other) as b:
         ya = a.MatMult_MFStokes_A11(xd).cpu().numpy()
         yb = b.MatMult_MFStokes_A11(xd).cpu().numpy()
         assert relerr(ya, yb) < 1e-14
