@@ -307,11 +307,9 @@ pt_status ensure_geometry(pt_op *op)
 pt_status ensure_ebe(pt_op *op)
 {
   if (op->ebe_valid) return PT_OK;
-  if (!op->d_Ae) {
-    PT_CUDA(op_alloc(op, (void **)&op->d_Ae, sizeof(double) * 6561 * op->nel));
-    PT_CUDA(op_alloc(op, (void **)&op->d_Ae32, sizeof(float) * 6561 * op->nel));
-    PT_CUDA(op_alloc(op, (void **)&op->d_ye, sizeof(double) * 81 * op->nel));
-  }
+  if (!op->d_Ae) PT_CUDA(op_alloc(op, (void **)&op->d_Ae, sizeof(double) * 6561 * op->nel));
+  if (!op->d_Ae32) PT_CUDA(op_alloc(op, (void **)&op->d_Ae32, sizeof(float) * 6561 * op->nel));
+  if (!op->d_ye) PT_CUDA(op_alloc(op, (void **)&op->d_ye, sizeof(double) * 81 * op->nel));
   ptk::element_matrix_kernel<double><<<(unsigned)op->nel, 96, 0, op->stream>>>(op->box, op->d_coords, op->d_eta,
                                                                                op->d_Ae);
   PT_LAUNCHED(op);
@@ -445,6 +443,16 @@ pt_status a21_d(pt_op *op, const double *u, double *yp, bool masked)
 
 pt_status a12_d(pt_op *op, const double *p, double *yu)
 {
+  if (op->a11_kernel == A11_EBE && op->full_box) {
+    // small box: element contributions in one launch, then the node gather
+    if (!op->d_ye) PT_CUDA(op_alloc(op, (void **)&op->d_ye, sizeof(double) * 81 * op->nel));
+    ptk::a12_elem_kernel<<<nblocks(op->nel), TPB, 0, op->stream>>>(op->box, op->d_coords, p, op->d_ye);
+    PT_LAUNCHED(op);
+    ptk::ebe_gather_kernel<double, false><<<grid_stride_blocks(op->nvel), 256, 0, op->stream>>>(op->box, op->d_ye,
+                                                                                               nullptr, nullptr, yu);
+    PT_LAUNCHED(op);
+    return PT_OK;
+  }
   PT_CUDA(cudaMemsetAsync(yu, 0, sizeof(double) * op->nvel, op->stream));
   for (int c = 0; c < 8; c++) {
     ptk::ColourGrid g = ptk::colour_grid(op->box, c);
