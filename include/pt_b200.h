@@ -307,6 +307,19 @@ pt_status pt_server_stats(const pt_server *server, int64_t *iterations, int64_t 
  * waiting for the device, and retiring. */
 pt_status pt_server_timers(const pt_server *server, double *enqueue, double *admit, double *wait, double *retire);
 
+/* ---- the whole Stokes operator ------------------------------------------- */
+
+/* Yu = A11 u + A12 p, Yp = A21 u as unassembled local sums, no BCs: replaces
+ * MFStokesWrapper_A / MFStokesWrapper_A_AVX (src/stokes_operators_mf.c:711-790,
+ * src/stokes_operators_avx.c:439-636).  Yu and Yp are overwritten. */
+pt_status pt_stokes_a_apply_d(pt_op *op, const double *u, const double *p, double *yu, double *yp);
+pt_status pt_stokes_a_apply_h(pt_op *op, const double *u, const double *p, double *yu, double *yp);
+/* MatMult_MFStokes_A (src/stokes_operators.c:893-979) on one rank: Dirichlet
+ * columns of xu zeroed, Yu = A11 xu + A12 xp, Yp = A21 xu, then Yu_k = xu_k on
+ * Dirichlet dofs (no pressure BCs, no surface constraints). */
+pt_status pt_matmult_a_d(pt_op *op, const double *xu, const double *xp, double *yu, double *yp);
+pt_status pt_matmult_a_h(pt_op *op, const double *xu, const double *xp, double *yu, double *yp);
+
 /* ---- selection, in the style of -a11_op --------------------------------- */
 
 /* Select the A11 kernel by name, like the reference's -a11_op function list

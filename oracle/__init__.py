@@ -135,6 +135,25 @@ class Oracle:
                                  _ptr(_f64(u)), _ptr(y))
         return y
 
+    # The whole Stokes operator (restated as the sum of its blocks, which is
+    # what MFStokesWrapper_A computes in one element loop:
+    # src/stokes_operators_mf.c:711-790, src/stokes_operators_avx.c:439-636)
+    def stokes_a(self, dims, coords, eta, u, p):
+        """Unassembled local Yu = A11 u + A12 p, Yp = A21 u (SpMVOp level)."""
+        yu = self.a11(dims, coords, eta, u) + self.a12(dims, coords, p)
+        return yu, self.a21(dims, coords, u)
+
+    def matmult_a(self, dims, coords, eta, mask, u, p):
+        """MatMult_MFStokes_A (src/stokes_operators.c:893-979): Dirichlet
+        columns of u zeroed, Yu = A11 u + A12 p, Yp = A21 u, then Yu_k = u_k on
+        Dirichlet dofs (no pressure BCs)."""
+        m = _mask(mask).astype(bool)
+        uz = _f64(u).copy()
+        uz[m] = 0.0
+        yu, yp = self.stokes_a(dims, coords, eta, uz, p)
+        yu[m] = _f64(u)[m]
+        return yu, yp
+
     def elements(self, dims):
         mx, my, mz = dims
         e = np.zeros(27 * mx * my * mz, dtype=np.int32)
@@ -169,6 +188,7 @@ class RefCPU:
         L.ref_diag.argtypes = [i, i, i, _dp, _dp, _dp]
         L.ref_a21.argtypes = [i, i, i, _dp, _dp, _dp]
         L.ref_a12.argtypes = [i, i, i, i, _dp, _dp, _dp]
+        L.ref_stokes_a.argtypes = [i, i, i, i, _dp, _dp, _dp, _dp, _dp, _dp]
         L.ref_has_avx.restype = i
 
     @staticmethod
@@ -192,6 +212,17 @@ class RefCPU:
         y = np.zeros(3 * (2 * mx + 1) * (2 * my + 1) * (2 * mz + 1))
         self._check(self.lib.ref_diag(mx, my, mz, _ptr(_f64(coords)), _ptr(_f64(eta)), _ptr(y)), "diag")
         return y
+
+    def stokes_a(self, dims, coords, eta, u, p, kind="avx"):
+        """Yu = A11 u + A12 p, Yp = A21 u (MFStokesWrapper_A[_AVX])."""
+        mx, my, mz = dims
+        u = _f64(u).copy()
+        p = _f64(p).copy()
+        yu = np.zeros_like(u)
+        yp = np.zeros_like(p)
+        self._check(self.lib.ref_stokes_a(self.KINDS[kind], mx, my, mz, _ptr(_f64(coords)), _ptr(_f64(eta)),
+                                          _ptr(u), _ptr(p), _ptr(yu), _ptr(yp)), "Stokes A")
+        return yu, yp
 
     def a21(self, dims, coords, u):
         mx, my, mz = dims

@@ -251,6 +251,25 @@ int ref_a12(int kind, int mx, int my, int mz, const double *coords, double *p, d
   return ierr;
 }
 
+/* The whole Stokes operator on one rank: Yu = A11 u + A12 p, Yp = A21 u
+ * (MFStokesWrapper_A_AVX, src/stokes_operators_avx.c:439-636, kind 1;
+ * MFStokesWrapper_A, src/stokes_operators_mf.c:711-790, kind 2). */
+int ref_stokes_a(int kind, int mx, int my, int mz, const double *coords, const double *eta, double *u, double *p,
+                 double *yu, double *yp)
+{
+  RefCtx c;
+  int ierr;
+  if (ctx_init(&c, mx, my, mz, coords, eta)) return 1;
+#if defined(__AVX__)
+  if (kind == 1) ierr = MFStokesWrapper_A_AVX(&c.volQ, &c.dau, u, &c.dap, p, yu, yp);
+  else
+#endif
+  if (kind == 2) ierr = MFStokesWrapper_A(&c.volQ, &c.dau, u, &c.dap, p, yu, yp);
+  else ierr = 2;
+  ctx_free(&c);
+  return ierr;
+}
+
 int ref_has_avx(void)
 {
 #if defined(__AVX__)

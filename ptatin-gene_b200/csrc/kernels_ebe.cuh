@@ -92,9 +92,9 @@ __global__ void __launch_bounds__(96) ebe_apply_kernel(Box b, const T *__restric
 }
 
 // y_k = sum over the (<= 8) elements of node k of their ye entry, in a fixed
-// order (MASKED: y_k = x_k on Dirichlet dofs).  One-rank boxes (node box =
-// element box).
-template <typename T, bool MASKED>
+// order (MASKED: y_k = x_k on Dirichlet dofs; ACC: added to y).  One-rank
+// boxes (node box = element box).
+template <typename T, bool MASKED, bool ACC = false>
 __global__ void ebe_gather_kernel(Box b, const T *__restrict__ ye, const T *__restrict__ x,
                                   const uint8_t *__restrict__ mask, T *__restrict__ y)
 {
@@ -131,7 +131,7 @@ __global__ void ebe_gather_kernel(Box b, const T *__restrict__ ye, const T *__re
           const int64_t e = ex[a] + (int64_t)b.mx * (ey[bb] + (int64_t)b.my * ez[c]);
           acc += ye[e * 81 + 3 * (lx[a] + 3 * ly[bb] + 9 * lz[c]) + l];
         }
-    y[t] = acc;
+    y[t] = ACC ? y[t] + acc : acc;
   }
 }
 

@@ -441,19 +441,24 @@ pt_status a21_d(pt_op *op, const double *u, double *yp, bool masked)
   return PT_OK;
 }
 
-pt_status a12_d(pt_op *op, const double *p, double *yu)
+// yu = B^T p, or yu += B^T p (accumulate)
+pt_status a12_d(pt_op *op, const double *p, double *yu, bool accumulate = false)
 {
   if (op->a11_kernel == A11_EBE && op->full_box) {
     // small box: element contributions in one launch, then the node gather
     if (!op->d_ye) PT_CUDA(op_alloc(op, (void **)&op->d_ye, sizeof(double) * 81 * op->nel));
     ptk::a12_elem_kernel<<<nblocks(op->nel), TPB, 0, op->stream>>>(op->box, op->d_coords, p, op->d_ye);
     PT_LAUNCHED(op);
-    ptk::ebe_gather_kernel<double, false><<<grid_stride_blocks(op->nvel), 256, 0, op->stream>>>(op->box, op->d_ye,
-                                                                                               nullptr, nullptr, yu);
+    if (accumulate)
+      ptk::ebe_gather_kernel<double, false, true><<<grid_stride_blocks(op->nvel), 256, 0, op->stream>>>(
+          op->box, op->d_ye, nullptr, nullptr, yu);
+    else
+      ptk::ebe_gather_kernel<double, false><<<grid_stride_blocks(op->nvel), 256, 0, op->stream>>>(
+          op->box, op->d_ye, nullptr, nullptr, yu);
     PT_LAUNCHED(op);
     return PT_OK;
   }
-  PT_CUDA(cudaMemsetAsync(yu, 0, sizeof(double) * op->nvel, op->stream));
+  if (!accumulate) PT_CUDA(cudaMemsetAsync(yu, 0, sizeof(double) * op->nvel, op->stream));
   for (int c = 0; c < 8; c++) {
     ptk::ColourGrid g = ptk::colour_grid(op->box, c);
     const int64_t n = (int64_t)g.ncx * g.ncy * g.ncz;
@@ -947,6 +952,65 @@ pt_status pt_matmult_a21_h(pt_op *op, const double *u, double *yp)
   if (s != PT_OK) return s;
   if ((s = ensure_staging(op)) != PT_OK) return s;
   return host_call(op, u, op->nvel, op->d_u, yp, op->npres, op->d_p, [&]() { return pt_matmult_a21_d(op, op->d_u, op->d_p); });
+}
+
+// ---- the whole Stokes operator ---------------------------------------------
+
+pt_status pt_stokes_a_apply_d(pt_op *op, const double *u, const double *p, double *yu, double *yp)
+{
+  pt_status s = check_ready(op, true);
+  if (s != PT_OK) return s;
+  if (!u || !p || !yu || !yp) return fail(PT_ERR_BAD_ARG, "NULL vector");
+  if (u == yu) return fail(PT_ERR_BAD_ARG, "u and yu must not alias");
+  if ((s = launch_a11<double>(op, op->d_coords, op->d_eta, u, yu, false)) != PT_OK) return s;
+  if ((s = a12_d(op, p, yu, true)) != PT_OK) return s;
+  return a21_d(op, u, yp, false);
+}
+
+pt_status pt_matmult_a_d(pt_op *op, const double *xu, const double *xp, double *yu, double *yp)
+{
+  pt_status s = check_ready(op, true);
+  if (s != PT_OK) return s;
+  if (!xu || !xp || !yu || !yp) return fail(PT_ERR_BAD_ARG, "NULL vector");
+  if (xu == yu) return fail(PT_ERR_BAD_ARG, "xu and yu must not alias");
+  // Dirichlet columns zeroed inside the masked kernels; rows set back to x after B^T p
+  if ((s = launch_a11<double>(op, op->d_coords, op->d_eta, xu, yu, op->has_mask)) != PT_OK) return s;
+  if ((s = a12_d(op, xp, yu, true)) != PT_OK) return s;
+  if ((s = bc_copy(op, xu, yu)) != PT_OK) return s;
+  return a21_d(op, xu, yp, op->has_mask);
+}
+
+static pt_status stokes_host(pt_op *op, const double *u, const double *p, double *yu, double *yp, bool matshell)
+{
+  pt_status s = check_ready(op, true);
+  if (s != PT_OK) return s;
+  if (!u || !p || !yu || !yp) return fail(PT_ERR_BAD_ARG, "NULL vector");
+  if ((s = ensure_staging(op)) != PT_OK) return s;
+  double *dyp = nullptr;
+  PT_CUDA(op_alloc(op, (void **)&dyp, sizeof(double) * op->npres));
+  cudaError_t e = cudaMemcpyAsync(op->d_u, u, sizeof(double) * op->nvel, cudaMemcpyHostToDevice, op->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(op->d_p, p, sizeof(double) * op->npres, cudaMemcpyHostToDevice, op->stream);
+  if (e == cudaSuccess) {
+    s = matshell ? pt_matmult_a_d(op, op->d_u, op->d_p, op->d_y, dyp) : pt_stokes_a_apply_d(op, op->d_u, op->d_p, op->d_y, dyp);
+    if (s == PT_OK) e = cudaMemcpyAsync(yu, op->d_y, sizeof(double) * op->nvel, cudaMemcpyDeviceToHost, op->stream);
+    if (s == PT_OK && e == cudaSuccess)
+      e = cudaMemcpyAsync(yp, dyp, sizeof(double) * op->npres, cudaMemcpyDeviceToHost, op->stream);
+    if (s == PT_OK && e == cudaSuccess) e = cudaStreamSynchronize(op->stream);
+  }
+  op_free(op, dyp);
+  if (s != PT_OK) return s;
+  if (e != cudaSuccess) return fail(PT_ERR_CUDA, "Stokes operator host call: %s", cudaGetErrorString(e));
+  return PT_OK;
+}
+
+pt_status pt_stokes_a_apply_h(pt_op *op, const double *u, const double *p, double *yu, double *yp)
+{
+  return stokes_host(op, u, p, yu, yp, false);
+}
+
+pt_status pt_matmult_a_h(pt_op *op, const double *xu, const double *xp, double *yu, double *yp)
+{
+  return stokes_host(op, xu, xp, yu, yp, true);
 }
 
 pt_status pt_op_set_a11_kernel(pt_op *op, const char *name)

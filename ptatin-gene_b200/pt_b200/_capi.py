@@ -90,6 +90,10 @@ SIGNATURES = {
     "pt_matmult_a12_d": [_vp, _vp, _vp],
     "pt_matmult_a21_h": [_vp, _vp, _vp],
     "pt_matmult_a21_d": [_vp, _vp, _vp],
+    "pt_stokes_a_apply_d": [_vp, _vp, _vp, _vp, _vp],
+    "pt_stokes_a_apply_h": [_vp, _vp, _vp, _vp, _vp],
+    "pt_matmult_a_d": [_vp, _vp, _vp, _vp, _vp],
+    "pt_matmult_a_h": [_vp, _vp, _vp, _vp, _vp],
     "pt_a11_apply_noalloc_d": [ctypes.POINTER(MeshDesc), _vp, _vp, _vp, _vp, _vp],
     "pt_solve_opts_default": [ctypes.POINTER(SolveOpts)],
     "pt_solver_create": [_vp, ctypes.POINTER(SolveOpts), ctypes.POINTER(_vp)],

@@ -223,6 +223,33 @@ class MatStokesMF:
         return self._apply("pt_a21_apply", Xu, self.npres, Yp)
 
     # -- MatShell level ------------------------------------------------------
+    def _apply2(self, base: str, u, p, Yu=None, Yp=None):
+        self._check_len(u, self.nvel, "u")
+        self._check_len(p, self.npres, "p")
+        if _is_dev(u):
+            Yu = torch.empty_like(u) if Yu is None else Yu
+            Yp = torch.empty(self.npres, dtype=torch.float64, device=u.device) if Yp is None else Yp
+            _capi.call(base + "_d", self._h, _dptr(u, torch.float64), _dptr(p, torch.float64),
+                       _dptr(Yu, torch.float64), _dptr(Yp, torch.float64))
+            return Yu, Yp
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        p = np.ascontiguousarray(p, dtype=np.float64)
+        Yu = np.empty(self.nvel) if Yu is None else Yu
+        Yp = np.empty(self.npres) if Yp is None else Yp
+        _capi.call(base + "_h", self._h, _hptr(u, np.float64), _hptr(p, np.float64), _hptr(Yu, np.float64),
+                   _hptr(Yp, np.float64))
+        return Yu, Yp
+
+    def MFStokesWrapper_A(self, ufield, pfield, Yu=None, Yp=None):
+        """The whole Stokes operator, unassembled and without BCs:
+        (A11 u + A12 p, A21 u) (MFStokesWrapper_A_AVX)."""
+        return self._apply2("pt_stokes_a_apply", ufield, pfield, Yu, Yp)
+
+    def MatMult_MFStokes_A(self, Xu, Xp, Yu=None, Yp=None):
+        """MatMult_MFStokes_A on one rank (Dirichlet columns zeroed, rows
+        copied); returns (Yu, Yp)."""
+        return self._apply2("pt_matmult_a", Xu, Xp, Yu, Yp)
+
     def MatMult_MFStokes_A11(self, X, Y=None):
         self._check_len(X, self.nvel, "X")
         if _is_dev(X) and X.dtype == torch.float32:

@@ -12,7 +12,11 @@ Each fixture stores the inputs and the reference outputs of
   diag(A11) (MFStokesWrapper_diagA11),
   A21 = B u (MFStokesWrapper_A21),
   A12 = B^T p via "avx" and "ref" (MFStokesWrapper_A12_AVX / MFStokesWrapper_A12),
+  the whole Stokes operator (Yu = A11 u + A12 p, Yp = A21 u) via "avx" and "ref"
+  (MFStokesWrapper_A_AVX / MFStokesWrapper_A),
 all as unassembled local sums on one rank (local == global numbering).
+The reference's OpenMP scatter ("omp critical") sums in thread order, so a
+re-run reproduces the A11 outputs only to ~1e-16 relative.
 """
 from __future__ import annotations
 
@@ -55,6 +59,8 @@ def make(name, workload, useed, pseed, refvec):
         a12_avx=r.a12(m.dims, m.coords, p, "avx"),
         a12_ref=r.a12(m.dims, m.coords, p, "ref"),
     )
+    out["a_u_avx"], out["a_p_avx"] = r.stokes_a(m.dims, m.coords, eta, uz, p, "avx")
+    out["a_u_ref"], out["a_p_ref"] = r.stokes_a(m.dims, m.coords, eta, uz, p, "ref")
     np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
 
 

@@ -59,3 +59,17 @@ def test_element_table_matches_reference_layout(ora):
     from pt_b200 import mesh as M
     for dims in [(1, 1, 1), (3, 2, 4), (5, 1, 2)]:
         assert np.array_equal(ora.elements(dims), M.element_table(*dims))
+
+
+@pytest.mark.parametrize("name", golden_names())
+def test_oracle_stokes_operator_matches_reference(ora, name):
+    """The whole Stokes operator (Yu = A11 u + A12 p, Yp = A21 u) of the
+    restatement against the reference's own MFStokesWrapper_A_AVX / _A."""
+    g = load_golden(name)
+    dims = tuple(int(v) for v in g["dims"])
+    uz = g["u"].copy()
+    uz[g["mask"].astype(bool)] = 0.0
+    yu, yp = ora.stokes_a(dims, g["coords"], g["eta"], uz, g["p"])
+    for kind in ("avx", "ref"):
+        assert relerr(yu, g["a_u_" + kind]) < 1e-13
+        assert relerr(yp, g["a_p_" + kind]) < 1e-13
