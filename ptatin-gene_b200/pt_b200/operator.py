@@ -51,11 +51,16 @@ def _dptr(t, dtype):
 class MatStokesMF:
     """One rank's Q2-P1disc Stokes operator on a structured box of mx*my*mz elements."""
 
-    def __init__(self, mx: int, my: int, mz: int, a11_op: str = "b200", stream=None):
+    def __init__(self, mx: int, my: int, mz: int, a11_op: str = "b200", stream=None, node_box=None):
+        """node_box = (nx, ny, nz, ox, oy, oz): the rank's ghosted local node box
+        and the offset of its first element's first node in it (the
+        DMDAGetGhostCorners / DMDAGetCornersElementQ2 layout of a multi-rank
+        run); None = a one-rank box."""
         self._lib = _capi.load()
         self.dims = (int(mx), int(my), int(mz))
         h = ctypes.c_void_p()
-        _capi.call("pt_op_create", ctypes.byref(_capi.MeshDesc(*self.dims)), ctypes.byref(h))
+        nb = tuple(int(v) for v in node_box) if node_box is not None else (0, 0, 0, 0, 0, 0)
+        _capi.call("pt_op_create", ctypes.byref(_capi.MeshDesc(*self.dims, *nb)), ctypes.byref(h))
         self._h = h
         nv, npr, nel = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64()
         _capi.call("pt_op_get_sizes", h, ctypes.byref(nv), ctypes.byref(npr), ctypes.byref(nel))

@@ -246,3 +246,48 @@ def test_matmult_stokes_a_matches_oracle(torch_cuda, ora, workload):
         assert np.array_equal(du.cpu().numpy(), yu) and np.array_equal(dp.cpu().numpy(), yp)
         bc = mask.astype(bool)
         assert np.array_equal(yu[bc], u[bc])
+
+
+@pytest.mark.parametrize("a11_op", ["b200", "b200_colour"])
+@pytest.mark.parametrize("part", [((1, 2), (0, 3), (2, 4)), ((0, 5), (1, 4), (0, 2)), ((2, 3), (0, 1), (1, 3))])
+def test_ghosted_rank_box_matches_oracle(torch_cuda, ora, part, a11_op):
+    """One rank of a multi-rank run: the op owns an element sub-box inside a
+    ghosted local node box (stencil width 2, clipped at the global boundary).
+    The SpMVOp-level applies read and write the ghosted local arrays and give
+    the owned elements' unassembled contributions, as the oracle on the
+    sub-box embedded in the ghosted box."""
+    from pt_b200 import MatStokesMF
+    torch = torch_cuda
+    m, eta, mask = M.problem("box:5,4,4", seed=41)
+    G = [2 * d + 1 for d in m.dims]                      # global nodes per axis
+    (ex0, ex1), (ey0, ey1), (ez0, ez1) = part            # owned elements [e0, e1)
+    lo = [max(0, 2 * e0 - 2) for e0 in (ex0, ey0, ez0)]  # ghosted node box
+    hi = [min(g, 2 * e1 + 1 + 2) for e1, g in zip((ex1, ey1, ez1), G)]
+    nb = [h - l for h, l in zip(hi, lo)]
+    off = [2 * e0 - l for e0, l in zip((ex0, ey0, ez0), lo)]
+    sub = (ex1 - ex0, ey1 - ey0, ez1 - ez0)
+    c = m.coords.reshape(G[2], G[1], G[0], 3)
+    cg = np.ascontiguousarray(c[lo[2]:hi[2], lo[1]:hi[1], lo[0]:hi[0]].reshape(-1))
+    e = eta.reshape(m.mz, m.my, m.mx, 27)[ez0:ez1, ey0:ey1, ex0:ex1].reshape(-1).copy()
+    u = M.uniform_vec(3 * nb[0] * nb[1] * nb[2], 42)
+    p = M.uniform_vec(4 * sub[0] * sub[1] * sub[2], 43)
+    # oracle: the sub-box on its own node block, embedded at the offset
+    ug = u.reshape(nb[2], nb[1], nb[0], 3)
+    sl = tuple(slice(o, o + 2 * n + 1) for o, n in zip(off[::-1], sub[::-1]))
+    cs = np.ascontiguousarray(cg.reshape(nb[2], nb[1], nb[0], 3)[sl].reshape(-1))
+    us = np.ascontiguousarray(ug[sl].reshape(-1))
+    ref_a11 = np.zeros_like(ug)
+    ref_a11[sl] = ora.a11(sub, cs, e, us).reshape(ref_a11[sl].shape)
+    ref_a12 = np.zeros_like(ug)
+    ref_a12[sl] = ora.a12(sub, cs, p).reshape(ref_a12[sl].shape)
+    with MatStokesMF(*sub, a11_op=a11_op, node_box=(*nb, *off)) as op:
+        op.set_coords(cg)
+        op.set_eta(e)
+        y = op.MFStokesWrapper_A11(torch.from_numpy(u).cuda()).cpu().numpy()
+        assert relerr(y, ref_a11.reshape(-1)) < TOL64
+        assert relerr(op.MFStokesWrapper_A21(u), ora.a21(sub, cs, us)) < TOL64
+        assert relerr(op.MFStokesWrapper_A12(p), ref_a12.reshape(-1)) < TOL64
+        d = op.MFStokesWrapper_diagA11()
+        dref = np.zeros_like(ug)
+        dref[sl] = ora.diag(sub, cs, e).reshape(dref[sl].shape)
+        assert relerr(d, dref.reshape(-1)) < TOL64
