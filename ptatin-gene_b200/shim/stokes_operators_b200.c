@@ -8,7 +8,9 @@
  *   MFA11Destroy_B200          -> MatA11MF->SpMVOp_Destroy
  * and provides drop-ins for the hard-wired diag / A12 / A21 element loops
  * (src/stokes_operators.c:1094, 1339-1343, 1479):
- *   MFStokesWrapper_diagA11_B200, MFStokesWrapper_A12_B200, MFStokesWrapper_A21_B200.
+ *   MFStokesWrapper_diagA11_B200, MFStokesWrapper_A12_B200, MFStokesWrapper_A21_B200,
+ * and for the whole Stokes operator of MatMult_MFStokes_A (stokes_operators.c:937-941):
+ *   MFStokesWrapper_A_B200.
  *
  * Contract, identical to the CPU back-ends (src/stokes_operators_tensor.c:181):
  * ufield/Xp/Xu are the rank's ghosted local arrays (Dirichlet entries already
@@ -223,6 +225,21 @@ PetscErrorCode MFStokesWrapper_A12_B200(Quadrature volQ, DM dau, DM dap, PetscSc
   (void)dap;
   ierr = B200_GetCached(dau, volQ, PETSC_FALSE, &c);CHKERRQ(ierr);
   PTCHK(pt_a12_apply_h(c->op, Xp, Yu));
+  PetscFunctionReturn(0);
+}
+
+/* Replaces MFStokesWrapper_A_AVX / MFStokesWrapper_A (stokes_operators_avx.c:439,
+ * stokes_operators_mf.c:711): Yu = A11 u + A12 p, Yp = A21 u in one call. */
+PetscErrorCode MFStokesWrapper_A_B200(Quadrature volQ, DM dau, PetscScalar ufield[], DM dap, PetscScalar pfield[],
+                                      PetscScalar Yu[], PetscScalar Yp[])
+{
+  PetscErrorCode ierr;
+  MFA11B200 *c;
+
+  PetscFunctionBeginUser;
+  (void)dap;
+  ierr = B200_GetCached(dau, volQ, PETSC_TRUE, &c);CHKERRQ(ierr);
+  PTCHK(pt_stokes_a_apply_h(c->op, ufield, pfield, Yu, Yp));
   PetscFunctionReturn(0);
 }
 
