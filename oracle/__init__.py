@@ -75,6 +75,7 @@ class Oracle:
         L.ora_matmult_a12.argtypes = [i, i, i, _dp, _u8p, _dp, _dp, i]
         L.ora_matmult_a21.argtypes = [i, i, i, _dp, _u8p, _dp, _dp]
         L.ora_a11_flops.argtypes = [ctypes.c_int64]
+        L.ora_marker_project.argtypes = [i, i, i, ctypes.c_int64, _i32p, _dp, _dp, _dp, _dp, _dp]
         L.ora_a11_flops.restype = ctypes.c_double
         L.ora_num_threads.restype = ctypes.c_int
 
@@ -154,6 +155,17 @@ class Oracle:
         yu[m] = _f64(u)[m]
         return yu, yp
 
+    def marker_project(self, dims, wil, xi, eta, rho):
+        """Gauss-point (eta, rho) from markers (restatement of the reference's
+        Q1 projection, src/material_point_utils.c:957-1190)."""
+        mx, my, mz = dims
+        w = np.ascontiguousarray(wil, dtype=np.int32)
+        eq = np.zeros(27 * mx * my * mz)
+        rq = np.zeros(27 * mx * my * mz)
+        self.lib.ora_marker_project(mx, my, mz, len(w), _ptr(w, _i32p), _ptr(_f64(xi)), _ptr(_f64(eta)),
+                                    _ptr(_f64(rho)), _ptr(eq), _ptr(rq))
+        return eq, rq
+
     def elements(self, dims):
         mx, my, mz = dims
         e = np.zeros(27 * mx * my * mz, dtype=np.int32)
@@ -189,6 +201,7 @@ class RefCPU:
         L.ref_a21.argtypes = [i, i, i, _dp, _dp, _dp]
         L.ref_a12.argtypes = [i, i, i, i, _dp, _dp, _dp]
         L.ref_stokes_a.argtypes = [i, i, i, i, _dp, _dp, _dp, _dp, _dp, _dp]
+        L.ref_marker_project.argtypes = [i, i, i, i, ctypes.POINTER(ctypes.c_int), _dp, _dp, _dp, _dp, _dp]
         L.ref_has_avx.restype = i
 
     @staticmethod
@@ -223,6 +236,18 @@ class RefCPU:
         self._check(self.lib.ref_stokes_a(self.KINDS[kind], mx, my, mz, _ptr(_f64(coords)), _ptr(_f64(eta)),
                                           _ptr(u), _ptr(p), _ptr(yu), _ptr(yp)), "Stokes A")
         return yu, yp
+
+    def marker_project(self, dims, wil, xi, eta, rho):
+        """Gauss-point (eta, rho) from markers by the reference's Q1 projection
+        (material_point_utils.c: _SwarmUpdateGaussPropertiesLocalL2ProjectionQ1_*)."""
+        mx, my, mz = dims
+        w = np.ascontiguousarray(wil, dtype=np.int32)
+        eq = np.zeros(27 * mx * my * mz)
+        rq = np.zeros(27 * mx * my * mz)
+        self._check(self.lib.ref_marker_project(mx, my, mz, len(w), w.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),
+                                                _ptr(_f64(xi)), _ptr(_f64(eta)), _ptr(_f64(rho)), _ptr(eq),
+                                                _ptr(rq)), "marker projection")
+        return eq, rq
 
     def a21(self, dims, coords, u):
         mx, my, mz = dims

@@ -689,6 +689,91 @@ void ora_matmult_a21(int mx, int my, int mz, const double *coords, const uint8_t
   free(ul);
 }
 
+/* ---- marker -> Gauss-point coefficients (Q1 projection) ------------------
+ * Restates src/material_point_utils.c:1090-1190 (_SwarmUpdateGauss
+ * PropertiesLocalL2ProjectionQ1_MPntPStokes_FineGrid) and :957-1088
+ * (..._InterpolateToQuadratePoints) on one rank:
+ *   node sums over the markers p of element wil[p], in marker order:
+ *     A1 += N_i eta_p, A2 += N_i rho_p, B += N_i, where N_i is the Q1 basis
+ *     (pTatinConstructNI_Q1_3D, :503-520) at xi_p on the 8 element vertices
+ *     (Q2 nodes 0,2,6,8,18,20,24,26) and 1 on the other 19 nodes;
+ *   A1 /= B, A2 /= B;
+ *   per element and Gauss point q: sum of the Q1 basis at xi_q times the
+ *   vertex values, clamped to [min, max] of the element's 27 node values.
+ * The Gauss abscissae are those of QuadratureCreateGauss_3pnt_3D
+ * (src/quadrature.c:136-167): +-0.774596669241483, 0. */
+static void q1_basis(const double xi[3], double N[8])
+{
+  const double x = xi[0], y = xi[1], z = xi[2];
+  N[0] = 0.125 * (1.0 - x) * (1.0 - y) * (1.0 - z);
+  N[1] = 0.125 * (1.0 + x) * (1.0 - y) * (1.0 - z);
+  N[2] = 0.125 * (1.0 - x) * (1.0 + y) * (1.0 - z);
+  N[3] = 0.125 * (1.0 + x) * (1.0 + y) * (1.0 - z);
+  N[4] = 0.125 * (1.0 - x) * (1.0 - y) * (1.0 + z);
+  N[5] = 0.125 * (1.0 + x) * (1.0 - y) * (1.0 + z);
+  N[6] = 0.125 * (1.0 - x) * (1.0 + y) * (1.0 + z);
+  N[7] = 0.125 * (1.0 + x) * (1.0 + y) * (1.0 + z);
+}
+
+static const int q1_vertex_node[8] = {0, 2, 6, 8, 18, 20, 24, 26};
+
+void ora_marker_project(int mx, int my, int mz, int64_t npoints, const int32_t *wil, const double *xi,
+                        const double *eta_p, const double *rho_p, double *eta_qp, double *rho_qp)
+{
+  const int64_t nel = (int64_t)mx * my * mz;
+  const int64_t nn = (int64_t)(2 * mx + 1) * (2 * my + 1) * (2 * mz + 1);
+  int32_t *el = (int32_t *)malloc(sizeof(int32_t) * 27 * (size_t)(nel > 0 ? nel : 1));
+  double *A1 = (double *)calloc((size_t)nn, sizeof(double));
+  double *A2 = (double *)calloc((size_t)nn, sizeof(double));
+  double *B = (double *)calloc((size_t)nn, sizeof(double));
+  const double g[3] = {-0.774596669241483, 0.0, 0.774596669241483};
+  if (!el || !A1 || !A2 || !B) goto done;
+  ora_elements_q2(mx, my, mz, el);
+  for (int64_t p = 0; p < npoints; p++) {
+    double N1[8], Ni[27];
+    q1_basis(&xi[3 * p], N1);
+    for (int i = 0; i < 27; i++) Ni[i] = 1.0;
+    for (int v = 0; v < 8; v++) Ni[q1_vertex_node[v]] = N1[v];
+    const int32_t *en = &el[27 * (int64_t)wil[p]];
+    for (int i = 0; i < 27; i++) {
+      A1[en[i]] += Ni[i] * eta_p[p];
+      A2[en[i]] += Ni[i] * rho_p[p];
+      B[en[i]] += Ni[i];
+    }
+  }
+  for (int64_t k = 0; k < nn; k++) {
+    A1[k] = A1[k] / B[k];
+    A2[k] = A2[k] / B[k];
+  }
+  for (int64_t e = 0; e < nel; e++) {
+    const int32_t *en = &el[27 * e];
+    double lo1 = 1.0e32, hi1 = -1.0e32, lo2 = 1.0e32, hi2 = -1.0e32;
+    for (int i = 0; i < 27; i++) {
+      if (A1[en[i]] < lo1) lo1 = A1[en[i]];
+      if (A1[en[i]] > hi1) hi1 = A1[en[i]];
+      if (A2[en[i]] < lo2) lo2 = A2[en[i]];
+      if (A2[en[i]] > hi2) hi2 = A2[en[i]];
+    }
+    for (int q = 0; q < 27; q++) {
+      const double xq[3] = {g[q % 3], g[(q / 3) % 3], g[q / 9]};
+      double N1[8], a = 0.0, b = 0.0;
+      q1_basis(xq, N1);
+      for (int v = 0; v < 8; v++) {
+        a += N1[v] * A1[en[q1_vertex_node[v]]];
+        b += N1[v] * A2[en[q1_vertex_node[v]]];
+      }
+      if (a < lo1) a = lo1;
+      if (a > hi1) a = hi1;
+      if (b < lo2) b = lo2;
+      if (b > hi2) b = hi2;
+      eta_qp[27 * e + q] = a;
+      rho_qp[27 * e + q] = b;
+    }
+  }
+done:
+  free(el); free(A1); free(A2); free(B);
+}
+
 double ora_a11_flops(int64_t nel)
 {
   return (double)nel * (9.0 * 3 * NQP * (6 + 6 + 6) + NQP * (14 + 1 + 27) + NQP * (5 * 9 + 6 + 6 + 6 * 9));

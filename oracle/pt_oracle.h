@@ -72,6 +72,10 @@ void ora_matmult_a21(int mx, int my, int mz, const double *coords, const uint8_t
                      const double *u, double *yp);
 
 /* Reference flop count of one tensor A11 apply (stokes_operators_tensor.c:279-281). */
+/* Marker -> Gauss-point (eta, rho), the reference's Q1 projection on one rank
+ * (src/material_point_utils.c:957-1190). */
+void ora_marker_project(int mx, int my, int mz, int64_t npoints, const int32_t *wil, const double *xi,
+                        const double *eta_p, const double *rho_p, double *eta_qp, double *rho_qp);
 double ora_a11_flops(int64_t nel);
 
 /* Number of OpenMP threads the element loops use (1 when built without OpenMP). */

@@ -19,6 +19,11 @@
  *     array of QPntVolCoefStokes built from a plain eta[27*nel].
  *   - PetscDTGaussQuadrature for n=3 (PETSc 3.8.3, absent here): closed form
  *     of the Golub-Welsch result, nodes 0, +-sqrt(3/5), weights 8/9, 5/9.
+ *   - for the marker -> Gauss-point viscosity projection of
+ *     src/material_point_utils.c: local vectors of a dof-1 Q2 node grid
+ *     (DMGetLocalVector ...), local<->global on one rank (identity / add),
+ *     VecPointwiseDivide, and the dof-1 element index / add-values helpers
+ *     (dmda_element_q2p1.c).
  */
 #include <petsc.h>
 #include <time.h>
@@ -29,15 +34,20 @@
 #include "dmda_element_q2p1.h"
 #include "stokes_operators.h"
 #include "stokes_operators_mf.h"
+#include "MPntStd_def.h"
+#include "MPntPStokes_def.h"
+#include "material_point_utils.h"
 
 struct _p_Vec {
   PetscScalar *a;
+  PetscInt n;
 };
 
 struct _p_DM {
   PetscInt nel, npe;
   PetscInt *elnidx;
   struct _p_Vec coords;
+  PetscInt nlocal; /* entries of a local (= global, one rank) vector */
 };
 
 PetscErrorCode PetscDTGaussQuadrature(PetscInt n, PetscReal a, PetscReal b, PetscReal *x, PetscReal *w)
@@ -140,6 +150,87 @@ PetscErrorCode VolumeQuadratureGetCellData_Stokes(Quadrature Q, QPntVolCoefStoke
 {
   if (cidx >= Q->n_elements) return PETSC_ERR_ARG_SIZ;
   *cell = &coeffs[cidx * Q->npoints];
+  return 0;
+}
+
+/* ---- vectors of a dof-1 node grid on one rank (local == global) ---------- */
+
+PetscErrorCode DMGetLocalVector(DM dm, Vec *v)
+{
+  struct _p_Vec *x = (struct _p_Vec *)calloc(1, sizeof *x);
+  if (!x) return PETSC_ERR_MEM;
+  x->n = dm->nlocal;
+  x->a = (PetscScalar *)calloc((size_t)(x->n > 0 ? x->n : 1), sizeof(PetscScalar));
+  if (!x->a) return PETSC_ERR_MEM;
+  *v = x;
+  return 0;
+}
+
+PetscErrorCode DMRestoreLocalVector(DM dm, Vec *v)
+{
+  (void)dm;
+  if (*v) {
+    free((*v)->a);
+    free(*v);
+  }
+  *v = NULL;
+  return 0;
+}
+
+PetscErrorCode VecZeroEntries(Vec v)
+{
+  memset(v->a, 0, sizeof(PetscScalar) * (size_t)v->n);
+  return 0;
+}
+
+PetscErrorCode DMLocalToGlobalBegin(DM dm, Vec l, InsertMode mode, Vec g)
+{
+  PetscInt i;
+  (void)dm;
+  for (i = 0; i < g->n; i++) g->a[i] = (mode == ADD_VALUES) ? g->a[i] + l->a[i] : l->a[i];
+  return 0;
+}
+
+PetscErrorCode DMLocalToGlobalEnd(DM dm, Vec l, InsertMode mode, Vec g)
+{
+  (void)dm; (void)l; (void)mode; (void)g;
+  return 0;
+}
+
+PetscErrorCode DMGlobalToLocalBegin(DM dm, Vec g, InsertMode mode, Vec l)
+{
+  PetscInt i;
+  (void)dm; (void)mode;
+  for (i = 0; i < l->n; i++) l->a[i] = g->a[i];
+  return 0;
+}
+
+PetscErrorCode DMGlobalToLocalEnd(DM dm, Vec g, InsertMode mode, Vec l)
+{
+  (void)dm; (void)g; (void)mode; (void)l;
+  return 0;
+}
+
+PetscErrorCode VecPointwiseDivide(Vec w, Vec x, Vec y)
+{
+  PetscInt i;
+  for (i = 0; i < w->n; i++) w->a[i] = x->a[i] / y->a[i];
+  return 0;
+}
+
+PetscErrorCode Q2GetElementLocalIndicesDOF(PetscInt el_localIndices[], PetscInt ndof, PetscInt elnid[])
+{
+  PetscInt n, d;
+  for (n = 0; n < 27; n++)
+    for (d = 0; d < ndof; d++) el_localIndices[ndof * n + d] = ndof * elnid[n] + d;
+  return 0;
+}
+
+PetscErrorCode DMDASetValuesLocalStencil_AddValues_DOF(PetscScalar *fields_F, PetscInt ndof, PetscInt eqn[],
+                                                       PetscScalar Fe[])
+{
+  PetscInt n;
+  for (n = 0; n < 27 * ndof; n++) fields_F[eqn[n]] += Fe[n];
   return 0;
 }
 
@@ -266,6 +357,66 @@ int ref_stokes_a(int kind, int mx, int my, int mz, const double *coords, const d
 #endif
   if (kind == 2) ierr = MFStokesWrapper_A(&c.volQ, &c.dau, u, &c.dap, p, yu, yp);
   else ierr = 2;
+  ctx_free(&c);
+  return ierr;
+}
+
+/* Marker -> Gauss-point viscosity and density, the reference's default Q1
+ * projection (coefficient_projection_type 1) on one level:
+ * _SwarmUpdateGaussPropertiesLocalL2ProjectionQ1_MPntPStokes_FineGrid and
+ * _SwarmUpdateGaussPropertiesLocalL2ProjectionQ1_MPntPStokes_InterpolateToQuadratePoints
+ * (src/material_point_utils.c:1090-1190, 957-1088).  Markers: element index
+ * wil, local coordinates xi[3], eta, rho.  Gauss points: the reference's
+ * QuadratureCreateGauss_3pnt_3D table (src/quadrature.c:136-167). */
+PetscErrorCode _SwarmUpdateGaussPropertiesLocalL2ProjectionQ1_MPntPStokes_FineGrid(DM, Vec, Vec, Vec, const int,
+                                                                                   MPntStd[], MPntPStokes[]);
+PetscErrorCode _SwarmUpdateGaussPropertiesLocalL2ProjectionQ1_MPntPStokes_InterpolateToQuadratePoints(
+    DM, Vec, Vec, Quadrature, SurfaceQuadrature, MeshFacetInfo);
+
+int ref_marker_project(int mx, int my, int mz, int npoints, const int *wil, const double *xi, const double *eta_p,
+                       const double *rho_p, double *eta_qp, double *rho_qp)
+{
+  RefCtx c;
+  int ierr = 0, p, k;
+  const double s = 0.774596669241483, xi1[3] = {-0.774596669241483, 0.0, 0.774596669241483};
+  PetscReal qxi[81];
+  struct _p_Vec A1, A2, B;
+  MPntStd *std = NULL;
+  MPntPStokes *stk = NULL;
+  (void)s;
+  if (ctx_init(&c, mx, my, mz, NULL, NULL)) return 1;
+  c.dau.nlocal = (PetscInt)(2 * mx + 1) * (2 * my + 1) * (2 * mz + 1);
+  for (k = 0; k < 27; k++) {
+    qxi[3 * k] = xi1[k % 3];
+    qxi[3 * k + 1] = xi1[(k / 3) % 3];
+    qxi[3 * k + 2] = xi1[k / 9];
+  }
+  c.volQ.q_xi_coor = qxi;
+  A1.n = A2.n = B.n = c.dau.nlocal;
+  A1.a = (PetscScalar *)calloc((size_t)A1.n, sizeof(PetscScalar));
+  A2.a = (PetscScalar *)calloc((size_t)A2.n, sizeof(PetscScalar));
+  B.a = (PetscScalar *)calloc((size_t)B.n, sizeof(PetscScalar));
+  std = (MPntStd *)calloc((size_t)(npoints > 0 ? npoints : 1), sizeof(MPntStd));
+  stk = (MPntPStokes *)calloc((size_t)(npoints > 0 ? npoints : 1), sizeof(MPntPStokes));
+  if (!A1.a || !A2.a || !B.a || !std || !stk) ierr = 1;
+  for (p = 0; !ierr && p < npoints; p++) {
+    std[p].pid = p;
+    std[p].wil = wil[p];
+    std[p].xi[0] = xi[3 * p]; std[p].xi[1] = xi[3 * p + 1]; std[p].xi[2] = xi[3 * p + 2];
+    stk[p].eta = eta_p[p];
+    stk[p].rho = rho_p[p];
+  }
+  if (!ierr) ierr = _SwarmUpdateGaussPropertiesLocalL2ProjectionQ1_MPntPStokes_FineGrid(&c.dau, &A1, &A2, &B, npoints,
+                                                                                        std, stk);
+  if (!ierr)
+    ierr = _SwarmUpdateGaussPropertiesLocalL2ProjectionQ1_MPntPStokes_InterpolateToQuadratePoints(&c.dau, &A1, &A2,
+                                                                                                  &c.volQ, NULL, NULL);
+  if (!ierr)
+    for (k = 0; k < 27 * mx * my * mz; k++) {
+      eta_qp[k] = c.qp[k].eta;
+      rho_qp[k] = c.qp[k].rho;
+    }
+  free(A1.a); free(A2.a); free(B.a); free(std); free(stk);
   ctx_free(&c);
   return ierr;
 }

@@ -18,6 +18,11 @@ typedef int MPI_Datatype;
 typedef int MPI_Op;
 typedef int MPI_Request;
 typedef int MPI_Win;
+typedef long MPI_Aint;
+#define MPI_DOUBLE 1
+int MPI_Get_address(const void *, MPI_Aint *);
+int MPI_Type_create_struct(int, const int *, const MPI_Aint *, const MPI_Datatype *, MPI_Datatype *);
+int MPI_Type_commit(MPI_Datatype *);
 typedef struct { int MPI_SOURCE, MPI_TAG, MPI_ERROR; } MPI_Status;
 #define MPI_COMM_WORLD 0
 #define MPI_COMM_SELF 1
@@ -35,6 +40,7 @@ typedef int64_t PetscInt64;
 typedef int64_t PetscObjectState;
 typedef enum { PETSC_FALSE = 0, PETSC_TRUE = 1 } PetscBool;
 typedef enum { INSERT_VALUES, ADD_VALUES } InsertMode;
+typedef enum { PETSC_VIEWER_DEFAULT, PETSC_VIEWER_ASCII_VTK } PetscViewerFormat;
 typedef enum { DM_BOUNDARY_NONE, DM_BOUNDARY_GHOSTED, DM_BOUNDARY_MIRROR, DM_BOUNDARY_PERIODIC } DMBoundaryType;
 typedef enum { DMDA_STENCIL_STAR, DMDA_STENCIL_BOX } DMDAStencilType;
 typedef enum { PETSC_COPY_VALUES, PETSC_OWN_POINTER, PETSC_USE_POINTER } PetscCopyMode;
@@ -83,6 +89,7 @@ typedef struct _p_PetscSF *PetscSF;
 #define PETSC_ERR_ARG_NULL 85
 #define PETSC_ERR_ARG_OUTOFRANGE 63
 #define PETSC_ERR_LIB 76
+#define PETSC_ERR_MEM 55
 #define PETSC_DECIDE -1
 #define PETSC_DEFAULT -2
 #define PETSC_NULL 0

@@ -243,6 +243,33 @@ def reference_test_vector(mesh: BoxMesh):
     return np.ascontiguousarray((s[:, None] + np.arange(3)[None, :] + 3.0).reshape(-1))
 
 
+def markers(mesh: BoxMesh, per_element=8, seed=1, contrast=1e4, n_incl=6, radius=0.15):
+    """Seeded material points: per_element markers per element at uniform
+    local coordinates, their physical positions through the Q2 map, and
+    viscosity 1 or `contrast` (inside n_incl spheres), density 1 + 0.1 eta^0.
+    Returns (wil int32[n], xi[n,3], x[n,3], eta[n], rho[n]); markers are
+    listed element by element in a seeded random order."""
+    rng = np.random.default_rng(seed)
+    nel = mesh.nel
+    wil = np.repeat(np.arange(nel, dtype=np.int32), per_element)
+    xi = rng.uniform(-1.0, 1.0, size=(wil.size, 3))
+    perm = rng.permutation(wil.size)
+    wil, xi = wil[perm], xi[perm]
+    # Q2 basis at the markers, physical coordinates
+    el = element_table(*mesh.dims)
+    c = mesh.coords.reshape(-1, 3)
+    Nx, Ny, Nz = (_q2_1d(xi[:, d]) for d in range(3))         # [3][n]
+    N = np.einsum("an,bn,cn->nabc", Nz, Ny, Nx).reshape(-1, 27)  # node a*9+b*3+c
+    x = np.einsum("nk,nkd->nd", N, c[el[wil]])
+    centres = rng.uniform(0.0, 1.0, size=(n_incl, 3))
+    inside = np.zeros(wil.size, dtype=bool)
+    for cc in centres:
+        inside |= ((x - cc) ** 2).sum(axis=1) < radius * radius
+    eta = np.where(inside, contrast, 1.0)
+    rho = 1.0 + 0.1 * inside
+    return wil.astype(np.int32), xi, x, eta, rho
+
+
 def problem(config: str, seed: int = 0):
     """Seeded inputs of a named box-mesh workload.
 

@@ -20,7 +20,14 @@ def pytest_configure(config):
 
 
 def golden_names():
-    return sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN_DIR, "*.npz")))
+    """Operator fixtures (inputs and the reference's A11/diag/B/B^T/A outputs)."""
+    return sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN_DIR, "*.npz"))
+                  if not os.path.basename(p).startswith("markers_"))
+
+
+def marker_golden_names():
+    """Marker -> Gauss-point projection fixtures."""
+    return sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN_DIR, "markers_*.npz")))
 
 
 def load_golden(name):

@@ -5,7 +5,8 @@ src/stokes_operators_{tensor,avx,mf}.c and src/element_utils_q{1,2}.c compiled
 unmodified (oracle/Makefile, Route A).  Inputs are seeded synthetic box meshes
 (ptatin-gene_b200/pt_b200/mesh.py).  Re-run after changing either:
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py          (markers fixtures; operator fixtures if absent)
+    python tests/golden/make_golden.py --all    (all fixtures)
 
 Each fixture stores the inputs and the reference outputs of
   A11 via "tensor", "avx" and "ref" (MFStokesWrapper_A11_*),
@@ -42,6 +43,23 @@ CASES = {
 }
 
 
+MARKER_CASES = {
+    # name: (workload, markers per element, seed)
+    "markers_c0_8x8x8": ("c0", 6, 51),
+    "markers_box_3x2x4": ("box:3,2,4", 11, 52),
+}
+
+
+def make_markers(name, workload, per_element, seed):
+    """Gauss-point (eta, rho) from seeded markers by the reference's Q1
+    projection (src/material_point_utils.c:957-1190)."""
+    m, _, _ = M.problem(workload)
+    wil, xi, x, eta, rho = M.markers(m, per_element, seed=seed)
+    eq, rq = oracle.RefCPU().marker_project(m.dims, wil, xi, eta, rho)
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), dims=np.array(m.dims, dtype=np.int32), wil=wil, xi=xi,
+                        eta=eta, rho=rho, eta_qp=eq, rho_qp=rq)
+
+
 def make(name, workload, useed, pseed, refvec):
     m, eta, mask = M.problem(workload)
     u = M.reference_test_vector(m) if refvec else M.uniform_vec(m.nvel, useed)
@@ -68,5 +86,9 @@ if __name__ == "__main__":
     if not oracle.RefCPU.available():
         oracle.build()
     for name, args in CASES.items():
-        make(name, *args)
+        if not os.path.exists(os.path.join(HERE, name + ".npz")) or "--all" in sys.argv:
+            make(name, *args)
+            print("wrote", name)
+    for name, args in MARKER_CASES.items():
+        make_markers(name, *args)
         print("wrote", name)

@@ -73,3 +73,16 @@ def test_oracle_stokes_operator_matches_reference(ora, name):
     for kind in ("avx", "ref"):
         assert relerr(yu, g["a_u_" + kind]) < 1e-13
         assert relerr(yp, g["a_p_" + kind]) < 1e-13
+
+
+@pytest.mark.parametrize("name", __import__("conftest").marker_golden_names())
+def test_oracle_marker_projection_matches_reference(ora, name):
+    """Marker -> Gauss-point (eta, rho) of the restatement against the
+    reference's own Q1 projection (src/material_point_utils.c, Route A)."""
+    g = load_golden(name)
+    dims = tuple(int(v) for v in g["dims"])
+    eq, rq = ora.marker_project(dims, g["wil"], g["xi"], g["eta"], g["rho"])
+    assert relerr(eq, g["eta_qp"]) < 1e-13
+    assert relerr(rq, g["rho_qp"]) < 1e-13
+    # values stay inside each element's node-value range (the clamp)
+    assert np.all(eq >= g["eta"].min() * (1 - 1e-12)) and np.all(eq <= g["eta"].max() * (1 + 1e-12))
