@@ -616,6 +616,52 @@ def run_serve(args):
     return 0
 
 
+def run_markers(args):
+    """Coefficient producer: Gauss-point (eta, rho) from material points by the
+    reference's Q1 projection, device-resident markers (CUDA events) and the
+    host path, against the reference's own CPU projection on the same markers."""
+    import torch
+
+    from pt_b200 import MatStokesMF
+    from pt_b200 import mesh as M
+    torch.cuda.set_device(0)
+    m, _, _ = M.problem(args.workload, seed=0)
+    wil, xi, _, eta, rho = M.markers(m, args.markers_per_element, seed=3)
+    n = len(wil)
+    op = MatStokesMF(*m.dims)
+    op.set_coords(m.coords)
+    dw, dx = torch.from_numpy(wil).cuda(), torch.from_numpy(xi).cuda()
+    de, dr = torch.from_numpy(eta).cuda(), torch.from_numpy(rho).cuda()
+    for _ in range(max(args.warmup, 3)):
+        op.ProjectMarkers(dw, dx, de, dr, install=False)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        op.ProjectMarkers(dw, dx, de, dr, install=False)
+    torch.cuda.synchronize()
+    t_dev = (time.perf_counter() - t0) / args.steps
+    t0 = time.perf_counter()
+    for _ in range(max(1, args.steps // 4)):
+        eq, rq = op.ProjectMarkers(wil, xi, eta, rho, install=False)
+    t_host = (time.perf_counter() - t0) / max(1, args.steps // 4)
+    out = {"mode": "markers", "workload": args.workload, "elements": m.nel, "markers": n,
+           "gpu_ms": t_dev * 1e3, "gpu_markers_per_s": n / t_dev, "e2e_ms": t_host * 1e3}
+    if not args.no_cpu_baseline:
+        import oracle
+        if not oracle.RefCPU.available():
+            oracle.build()
+        r = oracle.RefCPU()
+        t0 = time.perf_counter()
+        req, rrq = r.marker_project(m.dims, wil, xi, eta, rho)
+        t_cpu = time.perf_counter() - t0
+        rel = float(np.abs(eq - req).max() / np.abs(req).max())
+        out.update(cpu_ms=t_cpu * 1e3, cpu_kind="reference (material_point_utils.c, one thread: its loops are serial)",
+                   speedup=t_cpu / t_dev, relerr_vs_reference=rel)
+    op.Destroy()
+    print(json.dumps(out))
+    return 0
+
+
 def M_uniform(n, seed):
     return np.random.default_rng(seed).uniform(-1.0, 1.0, size=n)
 
@@ -632,7 +678,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", action="store_true", help="apply: keep the default tile schedule")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
-    ap.add_argument("--mode", default="apply", choices=["apply", "solve", "batched", "serve"])
+    ap.add_argument("--mode", default="apply", choices=["apply", "solve", "batched", "serve", "markers"])
+    ap.add_argument("--markers-per-element", type=int, default=8)
     ap.add_argument("--nreq", type=int, default=200, help="serve: requests in the measured stream")
     ap.add_argument("--ncal", type=int, default=48, help="serve: requests of the capacity calibration")
     ap.add_argument("--nserial", type=int, default=12, help="serve: requests solved one at a time")
@@ -651,6 +698,8 @@ def main():
         return run_batched(args)
     if args.mode == "serve":
         return run_serve(args)
+    if args.mode == "markers":
+        return run_markers(args)
     if args.impl == "reference":
         return run_reference(args)
     return run_ours(args)

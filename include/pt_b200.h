@@ -320,6 +320,25 @@ pt_status pt_stokes_a_apply_h(pt_op *op, const double *u, const double *p, doubl
 pt_status pt_matmult_a_d(pt_op *op, const double *xu, const double *xp, double *yu, double *yp);
 pt_status pt_matmult_a_h(pt_op *op, const double *xu, const double *xp, double *yu, double *yp);
 
+/* ---- Gauss-point coefficients from material points --------------------- */
+
+/* Viscosity and density at the Gauss points of the op's elements from
+ * material points, the reference's default projection
+ * (coefficient_projection_type 1, "Q1"): replaces
+ * _SwarmUpdateGaussPropertiesLocalL2ProjectionQ1_MPntPStokes_FineGrid and
+ * _SwarmUpdateGaussPropertiesLocalL2ProjectionQ1_MPntPStokes_InterpolateToQuadratePoints
+ * (src/material_point_utils.c:1090-1190, 957-1088) on one rank (the
+ * cross-rank sum of shared nodes is not included).  Markers: element index
+ * wil[n] within the op's element box (MPntStd.wil), local coordinates
+ * xi[3n] (MPntStd.xi), eta[n], rho[n] (MPntPStokes).  Outputs eta_qp,
+ * rho_qp [27 nel] in QPntVolCoefStokes order (either may be NULL); install != 0
+ * also sets eta_qp as the op's viscosity.  Deterministic (no atomics).
+ * PT_ERR_BAD_ARG if some wil lies outside the box (those markers are skipped). */
+pt_status pt_project_markers_d(pt_op *op, int64_t n, const int32_t *wil, const double *xi, const double *eta,
+                               const double *rho, double *eta_qp, double *rho_qp, int install);
+pt_status pt_project_markers_h(pt_op *op, int64_t n, const int32_t *wil, const double *xi, const double *eta,
+                               const double *rho, double *eta_qp, double *rho_qp, int install);
+
 /* ---- selection, in the style of -a11_op --------------------------------- */
 
 /* Select the A11 kernel by name, like the reference's -a11_op function list

@@ -1,0 +1,164 @@
+// Gauss-point viscosity and density from material points: the reference's
+// default coefficient projection (coefficient_projection_type 1, "Q1") on one
+// rank, src/material_point_utils.c:1090-1190 and 957-1088.
+//
+//   node sums over the markers of each element:  A1 += N_i eta_p,
+//   A2 += N_i rho_p, B += N_i, with N_i the Q1 basis at the marker's local
+//   coordinates on the element's 8 vertices (Q2 nodes 0,2,6,8,18,20,24,26)
+//   and 1 on its other 19 nodes;  A1 /= B, A2 /= B;  at each Gauss point the
+//   Q1 interpolant of the vertex values, clamped to the range of the
+//   element's 27 node values.
+//
+// Deterministic without atomics: markers are sorted by element (stable radix
+// sort, so each element keeps its markers in input order), one warp sums an
+// element's markers into per-element node partials (lane = node), and a
+// per-node gather adds the (<= 8) element partials in a fixed order.  Node
+// arrays are indexed compactly over the element box's own nodes.
+#pragma once
+
+#include <cstdint>
+
+namespace ptk {
+
+// Q1 basis of pTatinConstructNI_Q1_3D (src/material_point_utils.c:503-520),
+// vertex v = k*4 + j*2 + i.
+__device__ __forceinline__ double mk_q1(int v, double x, double y, double z)
+{
+  const double a = (v & 1) ? 1.0 + x : 1.0 - x;
+  const double b = (v & 2) ? 1.0 + y : 1.0 - y;
+  const double c = (v & 4) ? 1.0 + z : 1.0 - z;
+  return 0.125 * a * b * c;
+}
+
+// Q2 node of vertex v
+__device__ __forceinline__ int mk_vertex_node(int v) { return 2 * (v & 1) + 6 * ((v >> 1) & 1) + 18 * (v >> 2); }
+
+__global__ void mk_iota_kernel(int32_t *v, int64_t n)
+{
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    v[i] = (int32_t)i;
+}
+
+// start[e] = first sorted position with key >= e, e = 0..nel
+__global__ void mk_starts_kernel(const int32_t *__restrict__ keys, int64_t n, int64_t nel, int64_t *__restrict__ start)
+{
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e <= nel; e += (int64_t)gridDim.x * blockDim.x) {
+    int64_t lo = 0, hi = n;
+    while (lo < hi) {
+      const int64_t mid = (lo + hi) >> 1;
+      if (keys[mid] < e) lo = mid + 1;
+      else hi = mid;
+    }
+    start[e] = lo;
+  }
+}
+
+// One warp per element, lane i < 27 = node i: part[(e*27 + i)*3 + {0,1,2}] =
+// sums over the element's markers of (N_i eta, N_i rho, N_i).
+__global__ void __launch_bounds__(128) mk_element_kernel(int64_t nel, const int64_t *__restrict__ start,
+                                                         const int32_t *__restrict__ order,
+                                                         const double *__restrict__ xi, const double *__restrict__ eta,
+                                                         const double *__restrict__ rho, double *__restrict__ part)
+{
+  const int64_t e = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (e >= nel || lane >= 27) return;
+  // lane's vertex (or -1): nodes 0,2,6,8,18,20,24,26 are vertices 0..7
+  const int c = lane % 3, b = (lane / 3) % 3, a = lane / 9;
+  const int v = (c != 1 && b != 1 && a != 1) ? (c >> 1) + 2 * (b >> 1) + 4 * (a >> 1) : -1;
+  double s1 = 0.0, s2 = 0.0, sb = 0.0;
+  for (int64_t m = start[e]; m < start[e + 1]; m++) {
+    const int64_t p = order[m];
+    const double N = v >= 0 ? mk_q1(v, xi[3 * p], xi[3 * p + 1], xi[3 * p + 2]) : 1.0;
+    s1 += N * eta[p];
+    s2 += N * rho[p];
+    sb += N;
+  }
+  double *o = part + (e * 27 + lane) * 3;
+  o[0] = s1;
+  o[1] = s2;
+  o[2] = sb;
+}
+
+// Per node of the element box (compact index i + j X + k X Y, X = 2mx+1):
+// add the element partials in a fixed order, divide.
+__global__ void mk_node_kernel(int mx, int my, int mz, const double *__restrict__ part, double *__restrict__ v1,
+                               double *__restrict__ v2)
+{
+  const int X = 2 * mx + 1, Y = 2 * my + 1;
+  const int64_t nn = (int64_t)X * Y * (2 * mz + 1);
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < nn; t += (int64_t)gridDim.x * blockDim.x) {
+    const int i = (int)(t % X), j = (int)((t / X) % Y), k = (int)(t / ((int64_t)X * Y));
+    int ex[2], lx[2], nx = 0, ey[2], ly[2], ny = 0, ez[2], lz[2], nz = 0;
+    if (i & 1) { ex[0] = i >> 1; lx[0] = 1; nx = 1; }
+    else {
+      if (i > 0) { ex[nx] = (i >> 1) - 1; lx[nx++] = 2; }
+      if ((i >> 1) < mx) { ex[nx] = i >> 1; lx[nx++] = 0; }
+    }
+    if (j & 1) { ey[0] = j >> 1; ly[0] = 1; ny = 1; }
+    else {
+      if (j > 0) { ey[ny] = (j >> 1) - 1; ly[ny++] = 2; }
+      if ((j >> 1) < my) { ey[ny] = j >> 1; ly[ny++] = 0; }
+    }
+    if (k & 1) { ez[0] = k >> 1; lz[0] = 1; nz = 1; }
+    else {
+      if (k > 0) { ez[nz] = (k >> 1) - 1; lz[nz++] = 2; }
+      if ((k >> 1) < mz) { ez[nz] = k >> 1; lz[nz++] = 0; }
+    }
+    double a1 = 0.0, a2 = 0.0, b = 0.0;
+    for (int cz = 0; cz < nz; cz++)
+      for (int cy = 0; cy < ny; cy++)
+        for (int cx = 0; cx < nx; cx++) {
+          const int64_t e = ex[cx] + (int64_t)mx * (ey[cy] + (int64_t)my * ez[cz]);
+          const double *o = part + (e * 27 + lx[cx] + 3 * ly[cy] + 9 * lz[cz]) * 3;
+          a1 += o[0];
+          a2 += o[1];
+          b += o[2];
+        }
+    v1[t] = a1 / b;
+    v2[t] = a2 / b;
+  }
+}
+
+// Gauss point q of element e: Q1 interpolant of the vertex values, clamped to
+// the element's 27 node values.  Abscissae of QuadratureCreateGauss_3pnt_3D
+// (src/quadrature.c:136-167).
+__global__ void mk_qp_kernel(int mx, int my, int mz, const double *__restrict__ v1, const double *__restrict__ v2,
+                             double *__restrict__ eta_qp, double *__restrict__ rho_qp)
+{
+  const int64_t nel = (int64_t)mx * my * mz;
+  const int X = 2 * mx + 1, Y = 2 * my + 1;
+  const double g[3] = {-0.774596669241483, 0.0, 0.774596669241483};
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < nel * 27; t += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t e = t / 27;
+    const int q = (int)(t % 27);
+    const int ei = (int)(e % mx), ej = (int)((e / mx) % my), ek = (int)(e / ((int64_t)mx * my));
+    const int64_t base = 2 * (int64_t)ei + 2 * (int64_t)ej * X + 2 * (int64_t)ek * X * Y;
+    double lo1 = 1.0e32, hi1 = -1.0e32, lo2 = 1.0e32, hi2 = -1.0e32;
+    for (int n = 0; n < 27; n++) {
+      const int64_t nd = base + (n % 3) + ((n / 3) % 3) * (int64_t)X + (n / 9) * (int64_t)X * Y;
+      const double a = v1[nd], b = v2[nd];
+      if (a < lo1) lo1 = a;
+      if (a > hi1) hi1 = a;
+      if (b < lo2) lo2 = b;
+      if (b > hi2) hi2 = b;
+    }
+    const double x = g[q % 3], y = g[(q / 3) % 3], z = g[q / 9];
+    double s1 = 0.0, s2 = 0.0;
+    for (int v = 0; v < 8; v++) {
+      const int n = mk_vertex_node(v);
+      const int64_t nd = base + (n % 3) + ((n / 3) % 3) * (int64_t)X + (n / 9) * (int64_t)X * Y;
+      const double N = mk_q1(v, x, y, z);
+      s1 += N * v1[nd];
+      s2 += N * v2[nd];
+    }
+    if (s1 < lo1) s1 = lo1;
+    if (s1 > hi1) s1 = hi1;
+    if (s2 < lo2) s2 = lo2;
+    if (s2 > hi2) s2 = hi2;
+    if (eta_qp) eta_qp[t] = s1;
+    if (rho_qp) rho_qp[t] = s2;
+  }
+}
+
+}  // namespace ptk

@@ -24,6 +24,9 @@
 #include "kernels_stream.cuh"
 #include "kernels_tmem.cuh"
 #include "kernels_ebe.cuh"
+#include "kernels_markers.cuh"
+
+#include <cub/device/device_radix_sort.cuh>
 
 namespace {
 
@@ -1011,6 +1014,102 @@ pt_status pt_stokes_a_apply_h(pt_op *op, const double *u, const double *p, doubl
 pt_status pt_matmult_a_h(pt_op *op, const double *xu, const double *xp, double *yu, double *yp)
 {
   return stokes_host(op, xu, xp, yu, yp, true);
+}
+
+// ---- marker -> Gauss-point coefficients --------------------------------------
+
+pt_status pt_project_markers_d(pt_op *op, int64_t n, const int32_t *wil, const double *xi, const double *eta,
+                               const double *rho, double *eta_qp, double *rho_qp, int install)
+{
+  if (!op) return fail(PT_ERR_BAD_ARG, "op is NULL");
+  if (n < 0 || n > INT32_MAX) return fail(PT_ERR_BAD_ARG, "marker count must be in [0, 2^31)");
+  if (n > 0 && (!wil || !xi || !eta || !rho)) return fail(PT_ERR_BAD_ARG, "NULL marker array");
+  const cudaStream_t st = op->stream;
+  const int64_t nel = op->nel;
+  const int64_t nn = (int64_t)(2 * op->mx + 1) * (2 * op->my + 1) * (2 * op->mz + 1);
+  const int bits = 32;  // full key range: out-of-box indices sort to either end
+  // scratch, stream-ordered: sorted keys, order (2 x n), starts, element
+  // partials, node values, qp outputs when the caller passes none
+  int32_t *keys = nullptr, *iota = nullptr, *order = nullptr;
+  int64_t *start = nullptr;
+  double *part = nullptr, *v1 = nullptr, *eq = eta_qp, *rq = rho_qp;
+  void *tmp = nullptr;
+  size_t tmp_bytes = 0;
+  const int64_t nm = n > 0 ? n : 1;
+  cudaError_t e = cudaMallocAsync((void **)&keys, sizeof(int32_t) * nm, st);
+  if (e == cudaSuccess) e = cudaMallocAsync((void **)&iota, sizeof(int32_t) * nm, st);
+  if (e == cudaSuccess) e = cudaMallocAsync((void **)&order, sizeof(int32_t) * nm, st);
+  if (e == cudaSuccess) e = cudaMallocAsync((void **)&start, sizeof(int64_t) * (nel + 1), st);
+  if (e == cudaSuccess) e = cudaMallocAsync((void **)&part, sizeof(double) * 81 * nel, st);
+  if (e == cudaSuccess) e = cudaMallocAsync((void **)&v1, sizeof(double) * 2 * nn, st);
+  if (e == cudaSuccess && !eq) e = cudaMallocAsync((void **)&eq, sizeof(double) * 27 * nel, st);
+  if (e == cudaSuccess && n > 0) {
+    e = cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, wil, keys, iota, order, (int)n, 0, bits, st);
+    if (e == cudaSuccess) e = cudaMallocAsync(&tmp, tmp_bytes, st);
+  }
+  pt_status s = PT_OK;
+  if (e == cudaSuccess) {
+    if (n > 0) {
+      ptk::mk_iota_kernel<<<grid_stride_blocks(n), 256, 0, st>>>(iota, n);
+      e = cub::DeviceRadixSort::SortPairs(tmp, tmp_bytes, wil, keys, iota, order, (int)n, 0, bits, st);
+    }
+    if (e == cudaSuccess) {
+      ptk::mk_starts_kernel<<<grid_stride_blocks(nel + 1), 256, 0, st>>>(keys, n, nel, start);
+      ptk::mk_element_kernel<<<nblocks(32 * nel), TPB, 0, st>>>(nel, start, order, xi, eta, rho, part);
+      ptk::mk_node_kernel<<<grid_stride_blocks(nn), 256, 0, st>>>(op->mx, op->my, op->mz, part, v1, v1 + nn);
+      ptk::mk_qp_kernel<<<grid_stride_blocks(27 * nel), 256, 0, st>>>(op->mx, op->my, op->mz, v1, v1 + nn, eq, rq);
+      e = cudaGetLastError();
+      op->launches += 4 + (n > 0 ? 2 : 0);
+    }
+    // markers outside the element box are not projected: report them
+    int64_t edge[2] = {0, 0};
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&edge[0], start, sizeof(int64_t), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&edge[1], start + nel, sizeof(int64_t), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess && install) s = pt_op_set_eta_d(op, eq);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e == cudaSuccess && s == PT_OK && (edge[0] != 0 || edge[1] != n))
+      s = fail(PT_ERR_BAD_ARG, "%lld markers have an element index outside [0, %lld)",
+               (long long)(edge[0] + n - edge[1]), (long long)nel);
+  }
+  void *bufs[] = {keys, iota, order, start, part, v1, tmp, eq != eta_qp ? eq : nullptr};
+  for (void *b : bufs)
+    if (b) cudaFreeAsync(b, st);
+  if (e != cudaSuccess) return fail(PT_ERR_CUDA, "marker projection: %s", cudaGetErrorString(e));
+  return s;
+}
+
+pt_status pt_project_markers_h(pt_op *op, int64_t n, const int32_t *wil, const double *xi, const double *eta,
+                               const double *rho, double *eta_qp, double *rho_qp, int install)
+{
+  if (!op) return fail(PT_ERR_BAD_ARG, "op is NULL");
+  if (n < 0 || n > INT32_MAX) return fail(PT_ERR_BAD_ARG, "marker count must be in [0, 2^31)");
+  if (n > 0 && (!wil || !xi || !eta || !rho)) return fail(PT_ERR_BAD_ARG, "NULL marker array");
+  const cudaStream_t st = op->stream;
+  const int64_t nm = n > 0 ? n : 1, nq = 27 * op->nel;
+  int32_t *dw = nullptr;
+  double *dx = nullptr, *de = nullptr, *dr = nullptr, *deq = nullptr, *drq = nullptr;
+  cudaError_t e = cudaMallocAsync((void **)&dw, sizeof(int32_t) * nm, st);
+  if (e == cudaSuccess) e = cudaMallocAsync((void **)&dx, sizeof(double) * 3 * nm, st);
+  if (e == cudaSuccess) e = cudaMallocAsync((void **)&de, sizeof(double) * nm, st);
+  if (e == cudaSuccess) e = cudaMallocAsync((void **)&dr, sizeof(double) * nm, st);
+  if (e == cudaSuccess) e = cudaMallocAsync((void **)&deq, sizeof(double) * nq, st);
+  if (e == cudaSuccess) e = cudaMallocAsync((void **)&drq, sizeof(double) * nq, st);
+  if (e == cudaSuccess && n > 0) e = cudaMemcpyAsync(dw, wil, sizeof(int32_t) * n, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess && n > 0) e = cudaMemcpyAsync(dx, xi, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess && n > 0) e = cudaMemcpyAsync(de, eta, sizeof(double) * n, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess && n > 0) e = cudaMemcpyAsync(dr, rho, sizeof(double) * n, cudaMemcpyHostToDevice, st);
+  pt_status s = PT_OK;
+  if (e == cudaSuccess) s = pt_project_markers_d(op, n, dw, dx, de, dr, deq, drq, install);
+  if (e == cudaSuccess && s == PT_OK && eta_qp)
+    e = cudaMemcpyAsync(eta_qp, deq, sizeof(double) * nq, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess && s == PT_OK && rho_qp)
+    e = cudaMemcpyAsync(rho_qp, drq, sizeof(double) * nq, cudaMemcpyDeviceToHost, st);
+  void *bufs[] = {dw, dx, de, dr, deq, drq};
+  for (void *b : bufs)
+    if (b) cudaFreeAsync(b, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return fail(PT_ERR_CUDA, "marker projection: %s", cudaGetErrorString(e));
+  return s;
 }
 
 pt_status pt_op_set_a11_kernel(pt_op *op, const char *name)

@@ -94,6 +94,8 @@ SIGNATURES = {
     "pt_stokes_a_apply_h": [_vp, _vp, _vp, _vp, _vp],
     "pt_matmult_a_d": [_vp, _vp, _vp, _vp, _vp],
     "pt_matmult_a_h": [_vp, _vp, _vp, _vp, _vp],
+    "pt_project_markers_d": [_vp, ctypes.c_int64, _vp, _vp, _vp, _vp, _vp, _vp, ctypes.c_int],
+    "pt_project_markers_h": [_vp, ctypes.c_int64, _vp, _vp, _vp, _vp, _vp, _vp, ctypes.c_int],
     "pt_a11_apply_noalloc_d": [ctypes.POINTER(MeshDesc), _vp, _vp, _vp, _vp, _vp],
     "pt_solve_opts_default": [ctypes.POINTER(SolveOpts)],
     "pt_solver_create": [_vp, ctypes.POINTER(SolveOpts), ctypes.POINTER(_vp)],

@@ -245,6 +245,30 @@ class MatStokesMF:
                    _hptr(Yp, np.float64))
         return Yu, Yp
 
+    def ProjectMarkers(self, wil, xi, eta, rho, install=True):
+        """Gauss-point (eta, rho) from material points by the reference's Q1
+        projection (SwarmUpdateGaussPropertiesLocalL2Projection_Q1_MPntPStokes
+        on one rank); install=True also makes eta the op's viscosity.  Device
+        tensors in, device tensors out; numpy in, numpy out."""
+        n = len(wil)
+        if _is_dev(xi):
+            eq = torch.empty(27 * self.nel, dtype=torch.float64, device=xi.device)
+            rq = torch.empty_like(eq)
+            w = wil.to(torch.int32).contiguous()
+            _capi.call("pt_project_markers_d", self._h, n, ctypes.c_void_p(w.data_ptr()),
+                       _dptr(xi.reshape(-1), torch.float64), _dptr(eta, torch.float64), _dptr(rho, torch.float64),
+                       _dptr(eq, torch.float64), _dptr(rq, torch.float64), int(install))
+            return eq, rq
+        w = np.ascontiguousarray(wil, dtype=np.int32)
+        x = np.ascontiguousarray(xi, dtype=np.float64).reshape(-1)
+        e = np.ascontiguousarray(eta, dtype=np.float64)
+        r = np.ascontiguousarray(rho, dtype=np.float64)
+        eq = np.empty(27 * self.nel)
+        rq = np.empty(27 * self.nel)
+        _capi.call("pt_project_markers_h", self._h, n, w.ctypes.data, x.ctypes.data, e.ctypes.data, r.ctypes.data,
+                   eq.ctypes.data, rq.ctypes.data, int(install))
+        return eq, rq
+
     def MFStokesWrapper_A(self, ufield, pfield, Yu=None, Yp=None):
         """The whole Stokes operator, unassembled and without BCs:
         (A11 u + A12 p, A21 u) (MFStokesWrapper_A_AVX)."""

@@ -291,3 +291,39 @@ def test_ghosted_rank_box_matches_oracle(torch_cuda, ora, part, a11_op):
         dref = np.zeros_like(ug)
         dref[sl] = ora.diag(sub, cs, e).reshape(dref[sl].shape)
         assert relerr(d, dref.reshape(-1)) < TOL64
+
+
+@pytest.mark.parametrize("name", __import__("conftest").marker_golden_names())
+def test_marker_projection_matches_reference(torch_cuda, name):
+    """Gauss-point (eta, rho) from markers against the reference's own Q1
+    projection (src/material_point_utils.c); installing the result makes the
+    op's A11 equal to the oracle's with that viscosity."""
+    torch = torch_cuda
+    from pt_b200 import MatStokesMF
+    g = load_golden(name)
+    dims = tuple(int(v) for v in g["dims"])
+    m, _, mask = M.problem("c0" if dims == (8, 8, 8) else "box:%d,%d,%d" % dims)
+    with MatStokesMF(*dims) as op:
+        op.set_coords(m.coords)
+        eq, rq = op.ProjectMarkers(g["wil"], g["xi"], g["eta"], g["rho"])
+        assert relerr(eq, g["eta_qp"]) < TOL64 and relerr(rq, g["rho_qp"]) < TOL64
+        # device path, markers in another order: the same values
+        perm = np.random.default_rng(3).permutation(len(g["wil"]))
+        t = lambda a: torch.from_numpy(np.ascontiguousarray(a[perm])).cuda()
+        deq, drq = op.ProjectMarkers(t(g["wil"]), t(g["xi"]), t(g["eta"]), t(g["rho"]))
+        assert relerr(deq.cpu().numpy(), g["eta_qp"]) < TOL64
+        x = M.uniform_vec(m.nvel, 9)
+        y = op.MFStokesWrapper_A11(x)
+    from oracle import Oracle
+    assert relerr(y, Oracle().a11(dims, m.coords, deq.cpu().numpy(), x)) < TOL64
+
+
+def test_marker_projection_rejects_markers_outside_the_box(torch_cuda):
+    from pt_b200 import MatStokesMF, PtError
+    m, eta, mask = M.problem("box:3,2,2")
+    wil, xi, x, e, r = M.markers(m, 4, seed=5)
+    wil[7] = 12  # element count is 12
+    with MatStokesMF(*m.dims) as op:
+        op.set_coords(m.coords)
+        with pytest.raises(PtError, match="outside"):
+            op.ProjectMarkers(wil, xi, e, r, install=False)
