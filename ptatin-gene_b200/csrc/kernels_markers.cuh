@@ -54,7 +54,9 @@ __global__ void mk_starts_kernel(const int32_t *__restrict__ keys, int64_t n, in
 }
 
 // One warp per element, lane i < 27 = node i: part[(e*27 + i)*3 + {0,1,2}] =
-// sums over the element's markers of (N_i eta, N_i rho, N_i).
+// sums over the element's markers of (N_i eta, N_i rho, N_i).  The warp reads
+// up to 32 markers at a time (one per lane) and broadcasts them, so the sum
+// over markers runs in marker order without a chain of dependent loads.
 __global__ void __launch_bounds__(128) mk_element_kernel(int64_t nel, const int64_t *__restrict__ start,
                                                          const int32_t *__restrict__ order,
                                                          const double *__restrict__ xi, const double *__restrict__ eta,
@@ -62,22 +64,39 @@ __global__ void __launch_bounds__(128) mk_element_kernel(int64_t nel, const int6
 {
   const int64_t e = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
-  if (e >= nel || lane >= 27) return;
+  if (e >= nel) return;  // whole warp
   // lane's vertex (or -1): nodes 0,2,6,8,18,20,24,26 are vertices 0..7
   const int c = lane % 3, b = (lane / 3) % 3, a = lane / 9;
-  const int v = (c != 1 && b != 1 && a != 1) ? (c >> 1) + 2 * (b >> 1) + 4 * (a >> 1) : -1;
+  const int v = (lane < 27 && c != 1 && b != 1 && a != 1) ? (c >> 1) + 2 * (b >> 1) + 4 * (a >> 1) : -1;
   double s1 = 0.0, s2 = 0.0, sb = 0.0;
-  for (int64_t m = start[e]; m < start[e + 1]; m++) {
-    const int64_t p = order[m];
-    const double N = v >= 0 ? mk_q1(v, xi[3 * p], xi[3 * p + 1], xi[3 * p + 2]) : 1.0;
-    s1 += N * eta[p];
-    s2 += N * rho[p];
-    sb += N;
+  const int64_t m0 = start[e], m1 = start[e + 1];
+  for (int64_t c0 = m0; c0 < m1; c0 += 32) {
+    const int cnt = (int)min((int64_t)32, m1 - c0);
+    double x0 = 0.0, x1 = 0.0, x2 = 0.0, ee = 0.0, rr = 0.0;
+    if (lane < cnt) {
+      const int64_t p = order[c0 + lane];
+      x0 = xi[3 * p];
+      x1 = xi[3 * p + 1];
+      x2 = xi[3 * p + 2];
+      ee = eta[p];
+      rr = rho[p];
+    }
+    for (int k = 0; k < cnt; k++) {
+      const double y0 = __shfl_sync(0xffffffffu, x0, k), y1 = __shfl_sync(0xffffffffu, x1, k);
+      const double y2 = __shfl_sync(0xffffffffu, x2, k), ek = __shfl_sync(0xffffffffu, ee, k);
+      const double rk = __shfl_sync(0xffffffffu, rr, k);
+      const double N = v >= 0 ? mk_q1(v, y0, y1, y2) : 1.0;
+      s1 += N * ek;
+      s2 += N * rk;
+      sb += N;
+    }
   }
-  double *o = part + (e * 27 + lane) * 3;
-  o[0] = s1;
-  o[1] = s2;
-  o[2] = sb;
+  if (lane < 27) {
+    double *o = part + (e * 27 + lane) * 3;
+    o[0] = s1;
+    o[1] = s2;
+    o[2] = sb;
+  }
 }
 
 // Per node of the element box (compact index i + j X + k X Y, X = 2mx+1):
@@ -121,44 +140,50 @@ __global__ void mk_node_kernel(int mx, int my, int mz, const double *__restrict_
 }
 
 // Gauss point q of element e: Q1 interpolant of the vertex values, clamped to
-// the element's 27 node values.  Abscissae of QuadratureCreateGauss_3pnt_3D
+// the element's 27 node values.  One warp per element: lane n < 27 reads node
+// n once, the range is a warp reduction, the vertex values are broadcast, and
+// lane q writes Gauss point q.  Abscissae of QuadratureCreateGauss_3pnt_3D
 // (src/quadrature.c:136-167).
-__global__ void mk_qp_kernel(int mx, int my, int mz, const double *__restrict__ v1, const double *__restrict__ v2,
-                             double *__restrict__ eta_qp, double *__restrict__ rho_qp)
+__global__ void __launch_bounds__(128) mk_qp_kernel(int mx, int my, int mz, const double *__restrict__ v1,
+                                                    const double *__restrict__ v2, double *__restrict__ eta_qp,
+                                                    double *__restrict__ rho_qp)
 {
   const int64_t nel = (int64_t)mx * my * mz;
+  const int64_t e = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (e >= nel) return;  // whole warp
   const int X = 2 * mx + 1, Y = 2 * my + 1;
-  const double g[3] = {-0.774596669241483, 0.0, 0.774596669241483};
-  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < nel * 27; t += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t e = t / 27;
-    const int q = (int)(t % 27);
-    const int ei = (int)(e % mx), ej = (int)((e / mx) % my), ek = (int)(e / ((int64_t)mx * my));
-    const int64_t base = 2 * (int64_t)ei + 2 * (int64_t)ej * X + 2 * (int64_t)ek * X * Y;
-    double lo1 = 1.0e32, hi1 = -1.0e32, lo2 = 1.0e32, hi2 = -1.0e32;
-    for (int n = 0; n < 27; n++) {
-      const int64_t nd = base + (n % 3) + ((n / 3) % 3) * (int64_t)X + (n / 9) * (int64_t)X * Y;
-      const double a = v1[nd], b = v2[nd];
-      if (a < lo1) lo1 = a;
-      if (a > hi1) hi1 = a;
-      if (b < lo2) lo2 = b;
-      if (b > hi2) hi2 = b;
-    }
-    const double x = g[q % 3], y = g[(q / 3) % 3], z = g[q / 9];
-    double s1 = 0.0, s2 = 0.0;
-    for (int v = 0; v < 8; v++) {
-      const int n = mk_vertex_node(v);
-      const int64_t nd = base + (n % 3) + ((n / 3) % 3) * (int64_t)X + (n / 9) * (int64_t)X * Y;
-      const double N = mk_q1(v, x, y, z);
-      s1 += N * v1[nd];
-      s2 += N * v2[nd];
-    }
-    if (s1 < lo1) s1 = lo1;
-    if (s1 > hi1) s1 = hi1;
-    if (s2 < lo2) s2 = lo2;
-    if (s2 > hi2) s2 = hi2;
-    if (eta_qp) eta_qp[t] = s1;
-    if (rho_qp) rho_qp[t] = s2;
+  const int ei = (int)(e % mx), ej = (int)((e / mx) % my), ek = (int)(e / ((int64_t)mx * my));
+  const int64_t base = 2 * (int64_t)ei + 2 * (int64_t)ej * X + 2 * (int64_t)ek * X * Y;
+  // lanes 27..31 read node 0 again, so the range reduction needs no sentinel
+  const int n = lane < 27 ? lane : 0;
+  const int64_t nd = base + (n % 3) + ((n / 3) % 3) * (int64_t)X + (n / 9) * (int64_t)X * Y;
+  const double a = v1[nd], b = v2[nd];
+  double lo1 = a, hi1 = a, lo2 = b, hi2 = b;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    lo1 = fmin(lo1, __shfl_xor_sync(0xffffffffu, lo1, o));
+    hi1 = fmax(hi1, __shfl_xor_sync(0xffffffffu, hi1, o));
+    lo2 = fmin(lo2, __shfl_xor_sync(0xffffffffu, lo2, o));
+    hi2 = fmax(hi2, __shfl_xor_sync(0xffffffffu, hi2, o));
   }
+  const double g[3] = {-0.774596669241483, 0.0, 0.774596669241483};
+  const double x = g[n % 3], y = g[(n / 3) % 3], z = g[n / 9];
+  double s1 = 0.0, s2 = 0.0;
+#pragma unroll
+  for (int v = 0; v < 8; v++) {
+    const int vn = mk_vertex_node(v);
+    const double N = mk_q1(v, x, y, z);
+    s1 += N * __shfl_sync(0xffffffffu, a, vn);
+    s2 += N * __shfl_sync(0xffffffffu, b, vn);
+  }
+  if (lane >= 27) return;
+  if (s1 < lo1) s1 = lo1;
+  if (s1 > hi1) s1 = hi1;
+  if (s2 < lo2) s2 = lo2;
+  if (s2 > hi2) s2 = hi2;
+  if (eta_qp) eta_qp[27 * e + lane] = s1;
+  if (rho_qp) rho_qp[27 * e + lane] = s2;
 }
 
 }  // namespace ptk

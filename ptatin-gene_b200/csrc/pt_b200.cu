@@ -97,6 +97,9 @@ struct pt_op {
   double *d_Ae;
   float *d_Ae32;
   double *d_ye;
+  // marker projection scratch (grown on demand)
+  void *mk_scratch;
+  size_t mk_bytes;
   // pipelined host applies: copy streams and per-group events (created on first use)
   cudaStream_t h2d, d2h;
   cudaEvent_t ev_in[16], ev_done[16];
@@ -669,7 +672,8 @@ pt_status pt_op_destroy(pt_op *op)
   // pooled ops free in stream order (after the op's queued work); others wait
   if (op->stream && !op->pool) cudaStreamSynchronize(op->stream);
   void *bufs[] = {op->d_coords, op->d_eta, op->d_coords32, op->d_eta32, op->d_mask, op->d_u,
-                  op->d_y, op->d_p, op->d_K, op->d_K32, op->d_bad, op->d_Ae, op->d_Ae32, op->d_ye};
+                  op->d_y, op->d_p, op->d_K, op->d_K32, op->d_bad, op->d_Ae, op->d_Ae32, op->d_ye,
+                  op->mk_scratch};
   for (void *b : bufs) op_free(op, b);
   if (op->own_stream && op->stream) cudaStreamDestroy(op->stream);
   if (op->pipe_ready) {
@@ -1028,25 +1032,38 @@ pt_status pt_project_markers_d(pt_op *op, int64_t n, const int32_t *wil, const d
   const int64_t nel = op->nel;
   const int64_t nn = (int64_t)(2 * op->mx + 1) * (2 * op->my + 1) * (2 * op->mz + 1);
   const int bits = 32;  // full key range: out-of-box indices sort to either end
-  // scratch, stream-ordered: sorted keys, order (2 x n), starts, element
-  // partials, node values, qp outputs when the caller passes none
-  int32_t *keys = nullptr, *iota = nullptr, *order = nullptr;
-  int64_t *start = nullptr;
-  double *part = nullptr, *v1 = nullptr, *eq = eta_qp, *rq = rho_qp;
-  void *tmp = nullptr;
-  size_t tmp_bytes = 0;
+  // scratch (op-owned, grown on demand and reused): sorted keys, order (2 x n),
+  // starts, element partials, node values, qp outputs when the caller passes none
   const int64_t nm = n > 0 ? n : 1;
-  cudaError_t e = cudaMallocAsync((void **)&keys, sizeof(int32_t) * nm, st);
-  if (e == cudaSuccess) e = cudaMallocAsync((void **)&iota, sizeof(int32_t) * nm, st);
-  if (e == cudaSuccess) e = cudaMallocAsync((void **)&order, sizeof(int32_t) * nm, st);
-  if (e == cudaSuccess) e = cudaMallocAsync((void **)&start, sizeof(int64_t) * (nel + 1), st);
-  if (e == cudaSuccess) e = cudaMallocAsync((void **)&part, sizeof(double) * 81 * nel, st);
-  if (e == cudaSuccess) e = cudaMallocAsync((void **)&v1, sizeof(double) * 2 * nn, st);
-  if (e == cudaSuccess && !eq) e = cudaMallocAsync((void **)&eq, sizeof(double) * 27 * nel, st);
-  if (e == cudaSuccess && n > 0) {
-    e = cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, wil, keys, iota, order, (int)n, 0, bits, st);
-    if (e == cudaSuccess) e = cudaMallocAsync(&tmp, tmp_bytes, st);
+  size_t tmp_bytes = 0;
+  cudaError_t e = cudaSuccess;
+  if (n > 0)
+    e = cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, wil, (int32_t *)nullptr, (const int32_t *)nullptr,
+                                        (int32_t *)nullptr, (int)n, 0, bits, st);
+  if (e != cudaSuccess) return fail(PT_ERR_CUDA, "marker projection: %s", cudaGetErrorString(e));
+  auto up = [](size_t b) { return (b + 255) & ~(size_t)255; };
+  const size_t sz[8] = {up(4 * nm), up(4 * nm), up(4 * nm), up(8 * (nel + 1)), up(8 * 81 * nel), up(8 * 2 * nn),
+                        eta_qp ? 0 : up(8 * 27 * nel), up(tmp_bytes)};
+  size_t total = 0;
+  for (size_t b : sz) total += b;
+  if (total > op->mk_bytes) {
+    op_free(op, op->mk_scratch);
+    op->mk_scratch = nullptr;
+    op->mk_bytes = 0;
+    PT_CUDA(op_alloc(op, &op->mk_scratch, total));
+    op->mk_bytes = total;
   }
+  char *cur = (char *)op->mk_scratch;
+  void *ptrs[8];
+  for (int i = 0; i < 8; i++) {
+    ptrs[i] = sz[i] ? cur : nullptr;
+    cur += sz[i];
+  }
+  int32_t *keys = (int32_t *)ptrs[0], *iota = (int32_t *)ptrs[1], *order = (int32_t *)ptrs[2];
+  int64_t *start = (int64_t *)ptrs[3];
+  double *part = (double *)ptrs[4], *v1 = (double *)ptrs[5];
+  double *eq = eta_qp ? eta_qp : (double *)ptrs[6], *rq = rho_qp;
+  void *tmp = ptrs[7];
   pt_status s = PT_OK;
   if (e == cudaSuccess) {
     if (n > 0) {
@@ -1057,7 +1074,7 @@ pt_status pt_project_markers_d(pt_op *op, int64_t n, const int32_t *wil, const d
       ptk::mk_starts_kernel<<<grid_stride_blocks(nel + 1), 256, 0, st>>>(keys, n, nel, start);
       ptk::mk_element_kernel<<<nblocks(32 * nel), TPB, 0, st>>>(nel, start, order, xi, eta, rho, part);
       ptk::mk_node_kernel<<<grid_stride_blocks(nn), 256, 0, st>>>(op->mx, op->my, op->mz, part, v1, v1 + nn);
-      ptk::mk_qp_kernel<<<grid_stride_blocks(27 * nel), 256, 0, st>>>(op->mx, op->my, op->mz, v1, v1 + nn, eq, rq);
+      ptk::mk_qp_kernel<<<nblocks(32 * nel), TPB, 0, st>>>(op->mx, op->my, op->mz, v1, v1 + nn, eq, rq);
       e = cudaGetLastError();
       op->launches += 4 + (n > 0 ? 2 : 0);
     }
@@ -1071,9 +1088,6 @@ pt_status pt_project_markers_d(pt_op *op, int64_t n, const int32_t *wil, const d
       s = fail(PT_ERR_BAD_ARG, "%lld markers have an element index outside [0, %lld)",
                (long long)(edge[0] + n - edge[1]), (long long)nel);
   }
-  void *bufs[] = {keys, iota, order, start, part, v1, tmp, eq != eta_qp ? eq : nullptr};
-  for (void *b : bufs)
-    if (b) cudaFreeAsync(b, st);
   if (e != cudaSuccess) return fail(PT_ERR_CUDA, "marker projection: %s", cudaGetErrorString(e));
   return s;
 }
