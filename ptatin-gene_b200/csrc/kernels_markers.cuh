@@ -33,10 +33,17 @@ __device__ __forceinline__ double mk_q1(int v, double x, double y, double z)
 // Q2 node of vertex v
 __device__ __forceinline__ int mk_vertex_node(int v) { return 2 * (v & 1) + 6 * ((v >> 1) & 1) + 18 * (v >> 2); }
 
-__global__ void mk_iota_kernel(int32_t *v, int64_t n)
+// Sort keys and payload: key = element index, with every index outside
+// [0, nel) mapped to nel so that a radix sort over the bits of nel suffices;
+// payload = marker index.
+__global__ void mk_keys_kernel(const int32_t *__restrict__ wil, int64_t n, int32_t nel, int32_t *__restrict__ key,
+                               int32_t *__restrict__ idx)
 {
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-    v[i] = (int32_t)i;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t w = wil[i];
+    key[i] = (w >= 0 && w < nel) ? w : nel;
+    idx[i] = (int32_t)i;
+  }
 }
 
 // start[e] = first sorted position with key >= e, e = 0..nel
@@ -104,10 +111,12 @@ __global__ void __launch_bounds__(128) mk_element_kernel(int64_t nel, const int6
 __global__ void mk_node_kernel(int mx, int my, int mz, const double *__restrict__ part, double *__restrict__ v1,
                                double *__restrict__ v2)
 {
-  const int X = 2 * mx + 1, Y = 2 * my + 1;
-  const int64_t nn = (int64_t)X * Y * (2 * mz + 1);
-  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < nn; t += (int64_t)gridDim.x * blockDim.x) {
-    const int i = (int)(t % X), j = (int)((t / X) % Y), k = (int)(t / ((int64_t)X * Y));
+  // node count < 2^31 (checked by the caller): 32-bit index arithmetic
+  const unsigned X = 2 * mx + 1, Y = 2 * my + 1;
+  const unsigned nn = X * Y * (2 * mz + 1);
+  for (unsigned t = blockIdx.x * blockDim.x + threadIdx.x; t < nn; t += gridDim.x * blockDim.x) {
+    const unsigned txy = t / X;
+    const int i = (int)(t - txy * X), j = (int)(txy % Y), k = (int)(txy / Y);
     int ex[2], lx[2], nx = 0, ey[2], ly[2], ny = 0, ez[2], lz[2], nz = 0;
     if (i & 1) { ex[0] = i >> 1; lx[0] = 1; nx = 1; }
     else {
@@ -148,12 +157,14 @@ __global__ void __launch_bounds__(128) mk_qp_kernel(int mx, int my, int mz, cons
                                                     const double *__restrict__ v2, double *__restrict__ eta_qp,
                                                     double *__restrict__ rho_qp)
 {
-  const int64_t nel = (int64_t)mx * my * mz;
-  const int64_t e = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  // element count < 2^31 (checked by the caller): 32-bit index arithmetic
+  const unsigned nel = (unsigned)mx * my * mz;
+  const unsigned e = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (e >= nel) return;  // whole warp
   const int X = 2 * mx + 1, Y = 2 * my + 1;
-  const int ei = (int)(e % mx), ej = (int)((e / mx) % my), ek = (int)(e / ((int64_t)mx * my));
+  const unsigned exy = e / mx;
+  const int ei = (int)(e - exy * mx), ej = (int)(exy % my), ek = (int)(exy / my);
   const int64_t base = 2 * (int64_t)ei + 2 * (int64_t)ej * X + 2 * (int64_t)ek * X * Y;
   // lanes 27..31 read node 0 again, so the range reduction needs no sentinel
   const int n = lane < 27 ? lane : 0;
@@ -182,8 +193,8 @@ __global__ void __launch_bounds__(128) mk_qp_kernel(int mx, int my, int mz, cons
   if (s1 > hi1) s1 = hi1;
   if (s2 < lo2) s2 = lo2;
   if (s2 > hi2) s2 = hi2;
-  if (eta_qp) eta_qp[27 * e + lane] = s1;
-  if (rho_qp) rho_qp[27 * e + lane] = s2;
+  if (eta_qp) eta_qp[27 * (int64_t)e + lane] = s1;
+  if (rho_qp) rho_qp[27 * (int64_t)e + lane] = s2;
 }
 
 }  // namespace ptk

@@ -1031,19 +1031,24 @@ pt_status pt_project_markers_d(pt_op *op, int64_t n, const int32_t *wil, const d
   const cudaStream_t st = op->stream;
   const int64_t nel = op->nel;
   const int64_t nn = (int64_t)(2 * op->mx + 1) * (2 * op->my + 1) * (2 * op->mz + 1);
-  const int bits = 32;  // full key range: out-of-box indices sort to either end
-  // scratch (op-owned, grown on demand and reused): sorted keys, order (2 x n),
-  // starts, element partials, node values, qp outputs when the caller passes none
+  if (nn > INT32_MAX) return fail(PT_ERR_BAD_ARG, "marker projection: element box has 2^31 nodes or more");
+  // keys in [0, nel], nel standing for "outside the box": sort over nel's bits
+  int bits = 1;
+  while (bits < 31 && (int64_t(1) << bits) <= nel) bits++;
+  // scratch (op-owned, grown on demand and reused): keys in and sorted, marker
+  // indices in and sorted, starts, element partials, node values, qp outputs
+  // when the caller passes none, sort workspace
   const int64_t nm = n > 0 ? n : 1;
   size_t tmp_bytes = 0;
   cudaError_t e = cudaSuccess;
   if (n > 0)
-    e = cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, wil, (int32_t *)nullptr, (const int32_t *)nullptr,
-                                        (int32_t *)nullptr, (int)n, 0, bits, st);
+    e = cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, (const int32_t *)nullptr, (int32_t *)nullptr,
+                                        (const int32_t *)nullptr, (int32_t *)nullptr, (int)n, 0, bits, st);
   if (e != cudaSuccess) return fail(PT_ERR_CUDA, "marker projection: %s", cudaGetErrorString(e));
   auto up = [](size_t b) { return (b + 255) & ~(size_t)255; };
-  const size_t sz[8] = {up(4 * nm), up(4 * nm), up(4 * nm), up(8 * (nel + 1)), up(8 * 81 * nel), up(8 * 2 * nn),
-                        eta_qp ? 0 : up(8 * 27 * nel), up(tmp_bytes)};
+  const size_t sz[9] = {up(4 * nm),         up(4 * nm),     up(4 * nm),
+                        up(8 * (nel + 1)),   up(8 * 81 * nel), up(8 * 2 * nn),
+                        eta_qp ? 0 : up(8 * 27 * nel), up(tmp_bytes), up(4 * nm)};
   size_t total = 0;
   for (size_t b : sz) total += b;
   if (total > op->mk_bytes) {
@@ -1054,8 +1059,8 @@ pt_status pt_project_markers_d(pt_op *op, int64_t n, const int32_t *wil, const d
     op->mk_bytes = total;
   }
   char *cur = (char *)op->mk_scratch;
-  void *ptrs[8];
-  for (int i = 0; i < 8; i++) {
+  void *ptrs[9];
+  for (int i = 0; i < 9; i++) {
     ptrs[i] = sz[i] ? cur : nullptr;
     cur += sz[i];
   }
@@ -1064,11 +1069,12 @@ pt_status pt_project_markers_d(pt_op *op, int64_t n, const int32_t *wil, const d
   double *part = (double *)ptrs[4], *v1 = (double *)ptrs[5];
   double *eq = eta_qp ? eta_qp : (double *)ptrs[6], *rq = rho_qp;
   void *tmp = ptrs[7];
+  int32_t *kin = (int32_t *)ptrs[8];
   pt_status s = PT_OK;
   if (e == cudaSuccess) {
     if (n > 0) {
-      ptk::mk_iota_kernel<<<grid_stride_blocks(n), 256, 0, st>>>(iota, n);
-      e = cub::DeviceRadixSort::SortPairs(tmp, tmp_bytes, wil, keys, iota, order, (int)n, 0, bits, st);
+      ptk::mk_keys_kernel<<<grid_stride_blocks(n), 256, 0, st>>>(wil, n, (int32_t)nel, kin, iota);
+      e = cub::DeviceRadixSort::SortPairs(tmp, tmp_bytes, kin, keys, iota, order, (int)n, 0, bits, st);
     }
     if (e == cudaSuccess) {
       ptk::mk_starts_kernel<<<grid_stride_blocks(nel + 1), 256, 0, st>>>(keys, n, nel, start);
@@ -1078,15 +1084,15 @@ pt_status pt_project_markers_d(pt_op *op, int64_t n, const int32_t *wil, const d
       e = cudaGetLastError();
       op->launches += 4 + (n > 0 ? 2 : 0);
     }
-    // markers outside the element box are not projected: report them
-    int64_t edge[2] = {0, 0};
-    if (e == cudaSuccess) e = cudaMemcpyAsync(&edge[0], start, sizeof(int64_t), cudaMemcpyDeviceToHost, st);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(&edge[1], start + nel, sizeof(int64_t), cudaMemcpyDeviceToHost, st);
+    // markers outside the element box (key nel, sorted last) are not
+    // projected: report them
+    int64_t inside = 0;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&inside, start + nel, sizeof(int64_t), cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess && install) s = pt_op_set_eta_d(op, eq);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-    if (e == cudaSuccess && s == PT_OK && (edge[0] != 0 || edge[1] != n))
-      s = fail(PT_ERR_BAD_ARG, "%lld markers have an element index outside [0, %lld)",
-               (long long)(edge[0] + n - edge[1]), (long long)nel);
+    if (e == cudaSuccess && s == PT_OK && inside != n)
+      s = fail(PT_ERR_BAD_ARG, "%lld markers have an element index outside [0, %lld)", (long long)(n - inside),
+               (long long)nel);
   }
   if (e != cudaSuccess) return fail(PT_ERR_CUDA, "marker projection: %s", cudaGetErrorString(e));
   return s;

@@ -325,5 +325,9 @@ def test_marker_projection_rejects_markers_outside_the_box(torch_cuda):
     wil[7] = 12  # element count is 12
     with MatStokesMF(*m.dims) as op:
         op.set_coords(m.coords)
-        with pytest.raises(PtError, match="outside"):
+        with pytest.raises(PtError, match="1 markers have an element index outside"):
+            op.ProjectMarkers(wil, xi, e, r, install=False)
+        wil[3] = -1
+        wil[11] = 1 << 30
+        with pytest.raises(PtError, match="3 markers have an element index outside"):
             op.ProjectMarkers(wil, xi, e, r, install=False)
