@@ -312,12 +312,14 @@ __device__ __forceinline__ void stream_tile(const StreamGrid &g, int tx, int ej,
     const int sl[3] = {s0, s1, s2};
 
     if (active) {
+      // each quadrature plane's K is prefetched to L2 while the one before it computes
       const int64_t krow = kidx(row, 0, 0, g.MXP, ex);
+      const uint32_t kb = (uint32_t)(sizeof(T) * 81 * g.MXP);
+      if (t == 0) prefetch_k_plane(K + kidx(row, 9, 0, g.MXP, 0), kb);
       element_plane<T, TX, 0>(ut, yt, side, sl, t, warp, to_side, amask, K + krow, g.MXP);
-      if (t == 0) prefetch_k_plane(K + kidx(row, 18, 0, g.MXP, 0), (uint32_t)(sizeof(T) * 81 * g.MXP));
+      if (t == 0) prefetch_k_plane(K + kidx(row, 18, 0, g.MXP, 0), kb);
       element_plane<T, TX, 1>(ut, yt, side, sl, t, warp, to_side, amask, K + krow, g.MXP);
-      if (t == 0 && ek + 1 < ek1)
-        prefetch_k_plane(K + kidx(row + g.b.my, 0, 0, g.MXP, 0), (uint32_t)(sizeof(T) * 81 * g.MXP));
+      if (t == 0 && ek + 1 < ek1) prefetch_k_plane(K + kidx(row + g.b.my, 0, 0, g.MXP, 0), kb);
       element_plane<T, TX, 2>(ut, yt, side, sl, t, warp, to_side, amask, K + krow, g.MXP);
     }
     __syncthreads();
