@@ -199,9 +199,13 @@ typedef struct {
   int32_t mg_levels;    /* PT_PC_MG: levels (0 = coarsen while every axis is even and >= 4) */
   int32_t mg_coarse_degree; /* PT_PC_MG: Chebyshev steps on the coarsest level */
   int32_t pc_graph;     /* PT_PC_MG: replay the V-cycle as one captured CUDA graph */
-  int32_t mg_assembled; /* PT_PC_MG: levels of <= 32^3 elements keep element matrices and a
-                           coarsest level of <= 1200 dofs is solved by a dense inverse (1),
-                           or every level runs the matrix-free kernels (0) */
+  int32_t mg_assembled; /* PT_PC_MG coarse operators: 0 every level re-discretised and matrix-free;
+                           1 re-discretised, levels of <= 32^3 elements on stored element
+                           matrices and a coarsest level of <= 1200 dofs solved by a dense
+                           inverse; 2 as 1, and every level from the first one of <= 64^3
+                           elements down is Galerkin, P^T A P element by element
+                           (OP_TYPE_MFGALERKIN then OP_TYPE_GALERKIN,
+                           src/ptatin_driver_linear_ts.c:64-380, 713-800) */
 } pt_solve_opts;
 
 typedef struct {
@@ -219,7 +223,8 @@ typedef struct {
 typedef struct pt_solver pt_solver;
 
 /* Defaults: FGMRES(30), rtol 1e-8, max_it 10000, Chebyshev(3)-Jacobi in FP32,
- * window [0.2, 1.1], 20 Lanczos steps. */
+ * window [0.2, 1.1], 20 Lanczos steps; multigrid with Galerkin coarse levels
+ * (mg_assembled 2). */
 void pt_solve_opts_default(pt_solve_opts *opts);
 /* Allocates the Krylov workspace on the op's device. */
 pt_status pt_solver_create(pt_op *op, const pt_solve_opts *opts, pt_solver **solver);

@@ -277,6 +277,7 @@ struct pt_mg_level {
   void *x, *b, *r, *d, *az, *dl;  // T-sized work vectors
   void *t1, *t2;                   // transfer temporaries (to / from the next coarser level)
   void *Ae, *ye;                   // element matrices and per-element outputs (small levels), else null
+  double *Ae64;                    // Galerkin levels: FP64 element matrices P^T A P (Ae aliases or converts them)
   void *Ainv;                      // dense inverse (coarsest level, when small), else null
   int64_t nel;
 };

@@ -25,6 +25,7 @@
 #include "kernels_tmem.cuh"
 #include "kernels_ebe.cuh"
 #include "kernels_markers.cuh"
+#include "kernels_galerkin.cuh"
 
 #include <cub/device/device_radix_sort.cuh>
 

@@ -307,7 +307,8 @@ pt_status sv_setup_diag(pt_solver *s)
 // lambda_max(D^-1 A) of operator `op` (n dofs, inverse diagonal dinv) from
 // eig_its steps of Jacobi-PCG on a pseudo-random rhs (Lanczos tridiagonal).
 // Uses the solver's FP64 work vectors (fine-level size >= n).
-pt_status sv_lanczos(pt_solver *s, pt_op *op, int64_t n, const double *dinv, double *lmax)
+template <typename ApplyFn>
+pt_status sv_lanczos_fn(pt_solver *s, int64_t n, const double *dinv, double *lmax, ApplyFn apply)
 {
   double *b = s->t2, *p = s->t3, *q = s->w, *r = s->r, *z = s->t1;
   cudaStream_t st = s->op->stream;
@@ -321,8 +322,7 @@ pt_status sv_lanczos(pt_solver *s, pt_op *op, int64_t n, const double *dinv, dou
   if (stt != PT_OK) return stt;
   std::vector<double> alphas, betas, diag, off;
   for (int k = 0; k < s->o.eig_its && rz > 0.0; k++) {
-    if (op == s->op) s->n64++;
-    if ((stt = pt_matmult_a11_d(op, p, q)) != PT_OK) return stt;
+    if ((stt = apply(p, q)) != PT_OK) return stt;
     double pq;
     if ((stt = sv_dot(s, p, q, &pq, n)) != PT_OK) return stt;
     if (!(pq > 0.0)) break;
@@ -350,6 +350,14 @@ pt_status sv_lanczos(pt_solver *s, pt_op *op, int64_t n, const double *dinv, dou
   return PT_OK;
 }
 
+pt_status sv_lanczos(pt_solver *s, pt_op *op, int64_t n, const double *dinv, double *lmax)
+{
+  return sv_lanczos_fn(s, n, dinv, lmax, [&](const double *x, double *y) {
+    if (op == s->op) s->n64++;
+    return pt_matmult_a11_d(op, x, y);
+  });
+}
+
 pt_status sv_estimate_lambda(pt_solver *s) { return sv_lanczos(s, s->op, s->n, s->dinv, &s->lambda_max); }
 
 // ---- multigrid set-up -------------------------------------------------------
@@ -361,6 +369,7 @@ void mg_free(pt_mg *mg)
   for (pt_mg_level &L : mg->lv) {
     void *p[] = {L.dinv64, L.dinv32, L.x, L.b, L.r, L.d, L.az, L.dl, L.t1, L.Ae, L.ye, L.Ainv};
     for (void *q : p) cudaFree(q);
+    if (L.Ae64 && (void *)L.Ae64 != L.Ae) cudaFree(L.Ae64);
     if (L.own && L.op) pt_op_destroy(L.op);
   }
   delete mg;
@@ -406,16 +415,18 @@ pt_status mg_dense_inverse(pt_mg_level &L, bool fp32)
 {
   const pt_op *op = L.op;
   const int64_t n = L.n, nel = op->nel;
-  double *dAe = nullptr;
-  PT_CUDA(cudaMalloc(&dAe, sizeof(double) * 6561 * nel));
-  ptk::element_matrix_kernel<double><<<(unsigned)nel, 96, 0, op->stream>>>(op->box, op->d_coords, op->d_eta, dAe);
+  double *dAe = L.Ae64;  // Galerkin level: its own matrices; else re-discretised ones
+  if (!dAe) {
+    PT_CUDA(cudaMalloc(&dAe, sizeof(double) * 6561 * nel));
+    ptk::element_matrix_kernel<double><<<(unsigned)nel, 96, 0, op->stream>>>(op->box, op->d_coords, op->d_eta, dAe);
+  }
   std::vector<double> Ae(6561 * nel), A(n * n, 0.0);
   std::vector<uint8_t> mask(n);
   cudaError_t e = cudaGetLastError();
   if (e == cudaSuccess) e = cudaMemcpyAsync(Ae.data(), dAe, sizeof(double) * Ae.size(), cudaMemcpyDeviceToHost, op->stream);
   if (e == cudaSuccess) e = cudaMemcpyAsync(mask.data(), op->d_mask, n, cudaMemcpyDeviceToHost, op->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(op->stream);
-  cudaFree(dAe);
+  if (dAe != L.Ae64) cudaFree(dAe);
   if (e != cudaSuccess) return fail(PT_ERR_CUDA, "coarse element matrices: %s", cudaGetErrorString(e));
   const int64_t X = op->box.X, XY = op->box.XY;
   for (int64_t el = 0; el < nel; el++) {
@@ -490,10 +501,39 @@ pt_status mg_level_setup(pt_solver *s, pt_mg &mg, pt_mg_level &L, const pt_op *n
     PT_CUDA(cudaMalloc(&L.t1, 2 * ts * nt));
     L.t2 = (char *)L.t1 + ts * nt;
   }
-  pt_status st = pt_getdiag_a11_d(L.op, s->t1);
-  if (st != PT_OK) return st;
+  pt_status st = PT_OK;
+  if (L.Ae64) {
+    // Galerkin level: diagonal, lambda_max and applies from its element matrices
+    PT_CUDA(cudaMalloc(&L.ye, sizeof(double) * 81 * L.nel));
+    ptk::ebe_diag_kernel<<<vgrid(L.n), 256, 0, L.op->stream>>>(L.op->box, L.Ae64, s->t1);
+    PT_LAUNCHED(L.op);
+    if ((st = bc_value(L.op, 1.0, s->t1)) != PT_OK) return st;
+  } else if ((st = pt_getdiag_a11_d(L.op, s->t1)) != PT_OK) {
+    return st;
+  }
   reciprocal_kernel<<<vgrid(L.n), 256, 0, s->op->stream>>>(s->t1, L.dinv64, L.dinv32, L.n);
   PT_LAUNCHED(s->op);
+  if (L.Ae64) {
+    st = sv_lanczos_fn(s, L.n, L.dinv64, &L.lmax, [&](const double *x, double *y) {
+      ptk::ebe_apply_kernel<double, true><<<(unsigned)L.nel, 96, 0, L.op->stream>>>(L.op->box, L.Ae64, x,
+                                                                                     L.op->d_mask, (double *)L.ye);
+      PT_LAUNCHED(L.op);
+      ptk::ebe_gather_kernel<double, true><<<vgrid(L.n), 256, 0, L.op->stream>>>(L.op->box, (const double *)L.ye, x,
+                                                                                L.op->d_mask, y);
+      PT_LAUNCHED(L.op);
+      return PT_OK;
+    });
+    if (st != PT_OK) return st;
+    if (!next && L.n <= MG_DENSE_MAX_DOFS) return mg_dense_inverse(L, mg.fp32);
+    if (mg.fp32) {
+      PT_CUDA(cudaMalloc(&L.Ae, sizeof(float) * 6561 * L.nel));
+      ptk::convert_kernel<float><<<vgrid(6561 * L.nel), 256, 0, L.op->stream>>>(L.Ae64, (float *)L.Ae, 6561 * L.nel);
+      PT_LAUNCHED(L.op);
+    } else {
+      L.Ae = L.Ae64;
+    }
+    return PT_OK;
+  }
   if ((st = sv_lanczos(s, L.op, L.n, L.dinv64, &L.lmax)) != PT_OK) return st;
   if (!mg.assembled) return PT_OK;
   if (!next && L.n <= MG_DENSE_MAX_DOFS && (st = mg_dense_inverse(L, mg.fp32)) != PT_OK) return st;
@@ -507,6 +547,43 @@ pt_status mg_level_setup(pt_solver *s, pt_mg &mg, pt_mg_level &L, const pt_op *n
       ptk::element_matrix_kernel<double><<<(unsigned)L.nel, 96, 0, L.op->stream>>>(L.op->box, L.op->d_coords,
                                                                               L.op->d_eta, (double *)L.Ae);
     PT_LAUNCHED(L.op);
+  }
+  return PT_OK;
+}
+
+constexpr int64_t MG_GALERKIN_MAX_ELEMENTS = 262144;  // Galerkin levels up to 64^3 elements (13.8 GB FP64)
+
+// Galerkin coarse operators (mg_assembled = 2): every level from the first
+// one of <= MG_GALERKIN_MAX_ELEMENTS elements down gets element matrices
+// P^T A P from the level above -- from that level's quadrature when it runs
+// matrix-free (the reference's OP_TYPE_MFGALERKIN), from its Galerkin
+// matrices below that (OP_TYPE_GALERKIN).  Levels above stay re-discretised.
+pt_status mg_galerkin(pt_mg &mg)
+{
+  static bool attr_set[64] = {false};
+  int dev = 0;
+  PT_CUDA(cudaGetDevice(&dev));
+  constexpr size_t smem = ptk::galerkin_smem_bytes();
+  if (dev < 64 && !attr_set[dev]) {
+    PT_CUDA(cudaFuncSetAttribute(ptk::galerkin_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    PT_CUDA(cudaFuncSetAttribute(ptk::galerkin_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    attr_set[dev] = true;
+  }
+  for (size_t l = 1; l < mg.lv.size(); l++) {
+    pt_mg_level &F = mg.lv[l - 1], &C = mg.lv[l];
+    if (!F.Ae64 && C.op->nel > MG_GALERKIN_MAX_ELEMENTS) continue;
+    PT_CUDA(cudaMalloc(&C.Ae64, sizeof(double) * 6561 * C.op->nel));
+    ptk::GalerkinArgs a;
+    a.fb = F.op->box;
+    a.cmx = C.op->mx; a.cmy = C.op->my; a.cmz = C.op->mz;
+    a.coords = F.op->d_coords;
+    a.eta = F.op->d_eta;
+    a.Af = F.Ae64;
+    a.mask = F.op->has_mask ? F.op->d_mask : nullptr;
+    a.Ac = C.Ae64;
+    if (F.Ae64) ptk::galerkin_kernel<false><<<(unsigned)C.op->nel, ptk::GAL_THREADS, smem, C.op->stream>>>(a);
+    else ptk::galerkin_kernel<true><<<(unsigned)C.op->nel, ptk::GAL_THREADS, smem, C.op->stream>>>(a);
+    PT_LAUNCHED(C.op);
   }
   return PT_OK;
 }
@@ -550,10 +627,18 @@ pt_status mg_build(pt_solver *s)
   if (st == PT_OK && cudaStreamSynchronize(op->stream) != cudaSuccess) st = fail(PT_ERR_CUDA, "multigrid set-up failed");
   cudaFree(vf[0]);
   if (st != PT_OK) return st;
+  if (s->o.mg_assembled == 2 && (st = mg_galerkin(*mg)) != PT_OK) return st;
   for (size_t l = 0; l < mg->lv.size(); l++) {
     const pt_op *next = l + 1 < mg->lv.size() ? mg->lv[l + 1].op : nullptr;
     if ((st = mg_level_setup(s, *mg, mg->lv[l], next)) != PT_OK) return st;
   }
+  // FP32 smoothing keeps the FP32 copies only
+  if (mg->fp32)
+    for (pt_mg_level &L : mg->lv)
+      if (L.Ae64 && (void *)L.Ae64 != L.Ae) {
+        cudaFree(L.Ae64);
+        L.Ae64 = nullptr;
+      }
   s->lambda_max = mg->lv[0].lmax;
   return PT_OK;
 }
@@ -861,7 +946,7 @@ void pt_solve_opts_default(pt_solve_opts *o)
   o->mg_levels = 0;
   o->mg_coarse_degree = 24;
   o->pc_graph = 1;
-  o->mg_assembled = 1;
+  o->mg_assembled = 2;
 }
 
 pt_status pt_solver_create(pt_op *op, const pt_solve_opts *opts, pt_solver **out)
