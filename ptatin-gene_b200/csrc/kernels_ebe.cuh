@@ -2,13 +2,17 @@
 //
 // An element's 81x81 matrix is the colour kernel's element operator applied
 // to the unit vectors (exact FP64 arithmetic of the reference's element
-// kernel, adjugate form), stored column-major per element (Ae[e][j][i], j =
-// 3n+l the input dof) in FP64 or FP32.  An apply is two launches: a GEMV per
-// element into per-element outputs, and a gather per dof that sums the (at
-// most 8) element contributions of its node in a fixed order -- a node-
-// centred scatter, deterministic without atomics.  It reads 52 KB per
+// kernel, adjugate form), in FP64 or FP32.  The matrix is symmetric, so only
+// its upper triangle is stored, packed by columns: entry (i, j), i <= j, dof
+// index 3n+l, at j(j+1)/2 + i; 3321 values per element, padded to EBE_LD so
+// that each element's block starts on a 16-byte boundary.  An apply is two
+// launches: a GEMV per element into per-element outputs (the packed block
+// staged in shared memory by cp.async), and a gather per dof that sums the
+// (at most 8) element contributions of its node in a fixed order -- a node-
+// centred scatter, deterministic without atomics.  It reads 26.6 KB per
 // element (FP64), so it pays only where the streaming kernel is latency-bound
-// (small boxes: a few CTAs, each marching its layers one after another).
+// (small boxes: a few CTAs, each marching its layers one after another) and
+// on multigrid levels whose operator only exists as element matrices.
 #pragma once
 
 #include <cstdint>
@@ -17,6 +21,14 @@
 #include "q2_core.cuh"
 
 namespace ptk {
+
+constexpr int EBE_LD = 3328;  // packed upper triangle (3321) padded to a multiple of 16 bytes
+
+// Packed position of entry (i, j) of a symmetric element matrix.
+__host__ __device__ __forceinline__ int ebe_sym(int i, int j)
+{
+  return i <= j ? j * (j + 1) / 2 + i : i * (i + 1) / 2 + j;
+}
 
 
 // Column j of element e's matrix: the element operator of the colour kernel
@@ -57,23 +69,37 @@ __global__ void __launch_bounds__(96) element_matrix_kernel(Box b, const double 
     for (int k = 0; k < 3; k++)
       for (int l = 0; l < 3; l++) Ug[k][l][q] = d[k][l];
   }
-  T *col = Ae + (e * 81 + j) * 81;
+  T *blk = Ae + e * EBE_LD;
   for (int l = 0; l < 3; l++) {
     double r[27], f[27];
     q2::grad_colloc_t(Ug[0][l], Ug[1][l], Ug[2][l], r);
     q2::interp_t(r, f);
-    for (int n = 0; n < 27; n++) col[3 * n + l] = (T)f[n];
+    for (int n = 0; n < 27; n++)
+      if (3 * n + l <= j) blk[ebe_sym(3 * n + l, j)] = (T)f[n];
   }
+  if (j < EBE_LD - 3321) blk[3321 + j] = T(0);
 }
 
-// ye[e][i] = sum_j Ae[e][j][i] u_j (MASKED: Dirichlet entries of u taken as 0).
+// ye[e][i] = sum_j A_e(i, j) u_j in the order j = 0..80 (MASKED: Dirichlet
+// entries of u taken as 0).  The element's packed block is copied to shared
+// memory with 16-byte cp.async while u is gathered.
 template <typename T, bool MASKED>
 __global__ void __launch_bounds__(96) ebe_apply_kernel(Box b, const T *__restrict__ Ae, const T *__restrict__ u,
                                                        const uint8_t *__restrict__ mask, T *__restrict__ ye)
 {
+  __shared__ __align__(16) T S[EBE_LD];
   __shared__ T ue[81];
   const int t = threadIdx.x;
   const int64_t e = blockIdx.x;
+  {
+    constexpr int NCH = EBE_LD * (int)sizeof(T) / 16;
+    const char *src = reinterpret_cast<const char *>(Ae + e * EBE_LD);
+    const uint32_t dst = (uint32_t)__cvta_generic_to_shared(S);
+    for (int c = t; c < NCH; c += blockDim.x)
+      asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst + 16u * c), "l"(src + 16 * (int64_t)c)
+                   : "memory");
+    asm volatile("cp.async.commit_group;" ::: "memory");
+  }
   const int ei = (int)(e % b.mx), ej = (int)((e / b.mx) % b.my), ek = (int)(e / ((int64_t)b.mx * b.my));
   if (t < 81) {
     const int n = t / 3, l = t % 3;
@@ -81,12 +107,13 @@ __global__ void __launch_bounds__(96) ebe_apply_kernel(Box b, const T *__restric
     const int64_t k = 3 * node + l;
     ue[t] = (MASKED && mask[k]) ? T(0) : u[k];
   }
+  asm volatile("cp.async.wait_all;" ::: "memory");
   __syncthreads();
   if (t < 81) {
-    const T *A = Ae + e * 6561 + t;
+    const int pt = t * (t + 1) / 2;
     T acc = T(0);
 #pragma unroll 9
-    for (int jj = 0; jj < 81; jj++) acc = fma(A[jj * 81], ue[jj], acc);
+    for (int jj = 0; jj < 81; jj++) acc = fma(S[t <= jj ? jj * (jj + 1) / 2 + t : pt + jj], ue[jj], acc);
     ye[e * 81 + t] = acc;
   }
 }
@@ -166,7 +193,7 @@ __global__ void ebe_diag_kernel(Box b, const double *__restrict__ Ae, double *__
         for (int a = 0; a < nx; a++) {
           const int64_t e = ex[a] + (int64_t)b.mx * (ey[bb] + (int64_t)b.my * ez[c]);
           const int jj = 3 * (lx[a] + 3 * ly[bb] + 9 * lz[c]) + l;
-          acc += Ae[e * 6561 + (int64_t)jj * 81 + jj];
+          acc += Ae[e * EBE_LD + ebe_sym(jj, jj)];
         }
     d[t] = acc;
   }

@@ -21,13 +21,14 @@
 //     A[(n,a),(m,b)] = sum_q c_q (delta_ab g_n . g_m + g_n[b] g_m[a]),
 // the element matrix of 2 eta eps(u):eps(v).
 //
-// One CTA of 256 threads per coarse element; matrices column-major per
-// element (Ae[e][j][i], j = 3n+l the input dof), FP64.
+// One CTA of 256 threads per coarse element; matrices in the packed
+// symmetric layout of kernels_ebe.cuh, FP64.
 #pragma once
 
 #include <cstdint>
 
 #include "kernels_colour.cuh"
+#include "kernels_ebe.cuh"
 #include "q2_core.cuh"
 
 namespace ptk {
@@ -37,9 +38,9 @@ struct GalerkinArgs {
   int cmx, cmy, cmz;            // coarse level elements per axis
   const double *coords;         // MF: fine node coordinates
   const double *eta;            // MF: fine Gauss-point viscosity [27 nel_f]
-  const double *Af;             // !MF: fine element matrices [nel_f][81][81]
+  const double *Af;             // !MF: fine element matrices, packed [nel_f][EBE_LD]
   const uint8_t *mask;          // fine Dirichlet mask [3 N_f] or null
-  double *Ac;                   // out: coarse element matrices [nel_c][81][81]
+  double *Ac;                   // out: coarse element matrices, packed [nel_c][EBE_LD]
 };
 
 constexpr int GAL_THREADS = 256;
@@ -198,10 +199,10 @@ __global__ void __launch_bounds__(GAL_THREADS) galerkin_kernel(GalerkinArgs a)
           }
       }
     } else {
-      const double *src = a.Af + e * 6561;
+      const double *src = a.Af + e * EBE_LD;
       for (int idx = t; idx < 6561; idx += GAL_THREADS) {
         const int j = idx / 81, i = idx - 81 * j;
-        A[idx] = (mk[i] || mk[j]) ? 0.0 : src[idx];
+        A[idx] = (mk[i] || mk[j]) ? 0.0 : src[ebe_sym(i, j)];
       }
     }
     __syncthreads();
@@ -234,12 +235,15 @@ __global__ void __launch_bounds__(GAL_THREADS) galerkin_kernel(GalerkinArgs a)
     }
     __syncthreads();
   }
-  double *out = a.Ac + E * 6561;
+  // upper triangle, packed (the sum is symmetric up to rounding)
+  double *out = a.Ac + E * EBE_LD;
 #pragma unroll
   for (int k = 0; k < 26; k++) {
     const int idx = t + GAL_THREADS * k;
-    if (idx < 6561) out[idx] = acc[k];
+    const int j = idx / 81, i = idx - 81 * j;
+    if (idx < 6561 && i <= j) out[j * (j + 1) / 2 + i] = acc[k];
   }
+  if (t < EBE_LD - 3321) out[3321 + t] = 0.0;
 }
 
 template <typename TO>

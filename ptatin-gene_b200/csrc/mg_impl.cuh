@@ -305,6 +305,7 @@ pt_status mg_matmult(pt_mg &mg, pt_mg_level &L, const T *x, T *y)
   if (L.op == mg.lv[0].op) mg.fine_applies++;
   else mg.coarse_work += (double)L.op->nel / (double)mg.lv[0].op->nel;
   if (L.Ae) {
+    ebe_carveout<T, true>();
     ptk::ebe_apply_kernel<T, true><<<(unsigned)L.nel, 96, 0, L.op->stream>>>(L.op->box, (const T *)L.Ae, x,
                                                                               L.op->d_mask, (T *)L.ye);
     PT_LAUNCHED(L.op);

@@ -314,8 +314,8 @@ pt_status ensure_geometry(pt_op *op)
 pt_status ensure_ebe(pt_op *op)
 {
   if (op->ebe_valid) return PT_OK;
-  if (!op->d_Ae) PT_CUDA(op_alloc(op, (void **)&op->d_Ae, sizeof(double) * 6561 * op->nel));
-  if (!op->d_Ae32) PT_CUDA(op_alloc(op, (void **)&op->d_Ae32, sizeof(float) * 6561 * op->nel));
+  if (!op->d_Ae) PT_CUDA(op_alloc(op, (void **)&op->d_Ae, sizeof(double) * ptk::EBE_LD * op->nel));
+  if (!op->d_Ae32) PT_CUDA(op_alloc(op, (void **)&op->d_Ae32, sizeof(float) * ptk::EBE_LD * op->nel));
   if (!op->d_ye) PT_CUDA(op_alloc(op, (void **)&op->d_ye, sizeof(double) * 81 * op->nel));
   ptk::element_matrix_kernel<double><<<(unsigned)op->nel, 96, 0, op->stream>>>(op->box, op->d_coords, op->d_eta,
                                                                                op->d_Ae);
@@ -334,11 +334,26 @@ const double *op_Ae<double>(const pt_op *op) { return op->d_Ae; }
 template <>
 const float *op_Ae<float>(const pt_op *op) { return op->d_Ae32; }
 
+// The element GEMV stages 13-27 KB per CTA: ask for the largest shared-memory
+// carve-out so that 8 (FP64) to 16 (FP32) elements run per SM.
+template <typename T, bool MASKED>
+void ebe_carveout()
+{
+  static bool done[64] = {false};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev >= 64 || done[dev]) return;
+  cudaFuncSetAttribute(ptk::ebe_apply_kernel<T, MASKED>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                       (int)cudaSharedmemCarveoutMaxShared);
+  done[dev] = true;
+}
+
 template <typename T>
 pt_status launch_ebe(pt_op *op, const T *u, T *y, bool masked)
 {
   pt_status s = ensure_ebe(op);
   if (s != PT_OK) return s;
+  ebe_carveout<T, true>();
+  ebe_carveout<T, false>();
   T *ye = reinterpret_cast<T *>(op->d_ye);
   if (masked) {
     ptk::ebe_apply_kernel<T, true><<<(unsigned)op->nel, 96, 0, op->stream>>>(op->box, op_Ae<T>(op), u, op->d_mask, ye);

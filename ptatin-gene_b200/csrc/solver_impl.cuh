@@ -417,10 +417,10 @@ pt_status mg_dense_inverse(pt_mg_level &L, bool fp32)
   const int64_t n = L.n, nel = op->nel;
   double *dAe = L.Ae64;  // Galerkin level: its own matrices; else re-discretised ones
   if (!dAe) {
-    PT_CUDA(cudaMalloc(&dAe, sizeof(double) * 6561 * nel));
+    PT_CUDA(cudaMalloc(&dAe, sizeof(double) * ptk::EBE_LD * nel));
     ptk::element_matrix_kernel<double><<<(unsigned)nel, 96, 0, op->stream>>>(op->box, op->d_coords, op->d_eta, dAe);
   }
-  std::vector<double> Ae(6561 * nel), A(n * n, 0.0);
+  std::vector<double> Ae(ptk::EBE_LD * nel), A(n * n, 0.0);
   std::vector<uint8_t> mask(n);
   cudaError_t e = cudaGetLastError();
   if (e == cudaSuccess) e = cudaMemcpyAsync(Ae.data(), dAe, sizeof(double) * Ae.size(), cudaMemcpyDeviceToHost, op->stream);
@@ -436,11 +436,11 @@ pt_status mg_dense_inverse(pt_mg_level &L, bool fp32)
       const int64_t node = (2 * ei + nn % 3) + (2 * ej + (nn / 3) % 3) * X + (2 * ek + nn / 9) * XY;
       for (int l = 0; l < 3; l++) g[3 * nn + l] = 3 * node + l;
     }
-    const double *m = &Ae[el * 6561];
+    const double *m = &Ae[el * ptk::EBE_LD];
     for (int jj = 0; jj < 81; jj++) {
       if (mask[g[jj]]) continue;
       for (int ii = 0; ii < 81; ii++)
-        if (!mask[g[ii]]) A[g[ii] * n + g[jj]] += m[jj * 81 + ii];
+        if (!mask[g[ii]]) A[g[ii] * n + g[jj]] += m[ptk::ebe_sym(ii, jj)];
     }
   }
   for (int64_t i = 0; i < n; i++)
@@ -526,8 +526,9 @@ pt_status mg_level_setup(pt_solver *s, pt_mg &mg, pt_mg_level &L, const pt_op *n
     if (st != PT_OK) return st;
     if (!next && L.n <= MG_DENSE_MAX_DOFS) return mg_dense_inverse(L, mg.fp32);
     if (mg.fp32) {
-      PT_CUDA(cudaMalloc(&L.Ae, sizeof(float) * 6561 * L.nel));
-      ptk::convert_kernel<float><<<vgrid(6561 * L.nel), 256, 0, L.op->stream>>>(L.Ae64, (float *)L.Ae, 6561 * L.nel);
+      PT_CUDA(cudaMalloc(&L.Ae, sizeof(float) * ptk::EBE_LD * L.nel));
+      ptk::convert_kernel<float><<<vgrid(ptk::EBE_LD * L.nel), 256, 0, L.op->stream>>>(L.Ae64, (float *)L.Ae,
+                                                                                     ptk::EBE_LD * L.nel);
       PT_LAUNCHED(L.op);
     } else {
       L.Ae = L.Ae64;
@@ -538,7 +539,7 @@ pt_status mg_level_setup(pt_solver *s, pt_mg &mg, pt_mg_level &L, const pt_op *n
   if (!mg.assembled) return PT_OK;
   if (!next && L.n <= MG_DENSE_MAX_DOFS && (st = mg_dense_inverse(L, mg.fp32)) != PT_OK) return st;
   if (L.nel <= MG_EBE_MAX_ELEMENTS && !L.Ainv) {
-    PT_CUDA(cudaMalloc(&L.Ae, ts * 6561 * L.nel));
+    PT_CUDA(cudaMalloc(&L.Ae, ts * ptk::EBE_LD * L.nel));
     PT_CUDA(cudaMalloc(&L.ye, ts * 81 * L.nel));
     if (mg.fp32)
       ptk::element_matrix_kernel<float><<<(unsigned)L.nel, 96, 0, L.op->stream>>>(L.op->box, L.op->d_coords, L.op->d_eta,
@@ -572,7 +573,7 @@ pt_status mg_galerkin(pt_mg &mg)
   for (size_t l = 1; l < mg.lv.size(); l++) {
     pt_mg_level &F = mg.lv[l - 1], &C = mg.lv[l];
     if (!F.Ae64 && C.op->nel > MG_GALERKIN_MAX_ELEMENTS) continue;
-    PT_CUDA(cudaMalloc(&C.Ae64, sizeof(double) * 6561 * C.op->nel));
+    PT_CUDA(cudaMalloc(&C.Ae64, sizeof(double) * ptk::EBE_LD * C.op->nel));
     ptk::GalerkinArgs a;
     a.fb = F.op->box;
     a.cmx = C.op->mx; a.cmy = C.op->my; a.cmz = C.op->mz;
