@@ -78,3 +78,19 @@ def test_server_option_validation_without_device():
     h = ctypes.c_void_p()
     assert lib.pt_server_create(ctypes.byref(o), ctypes.byref(h)) == 1
     assert b"max_active" in lib.pt_last_error()
+
+
+def test_solver_defaults_without_device():
+    """pt_solve_opts_default: FGMRES(30), rtol 1e-8, Chebyshev(3)-Jacobi in FP32
+    over [0.2, 1.1] lambda_max (the reference's esteig window), Galerkin
+    coarse levels."""
+    from pt_b200 import _capi
+    from pt_b200.solver import KSP, PC
+    lib = _capi.load()
+    o = _capi.SolveOpts()
+    lib.pt_solve_opts_default(ctypes.byref(o))
+    assert o.ksp == KSP["fgmres"] and o.restart == 30 and o.rtol == 1e-8
+    assert o.cheby_degree == 3 and o.cheby_fp32 == 1
+    assert (o.cheby_emin, o.cheby_emax) == (0.2, 1.1)
+    assert o.mg_assembled == 2 and o.pc_graph == 1
+    assert PC["mg"] == 3
