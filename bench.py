@@ -155,12 +155,12 @@ def max_over_ranks(x, pg, device):
 
 
 def barrier(pg, device):
+    import torch
     if pg is not None:
-        import torch
         t = torch.zeros(1, device=device)
         pg.all_reduce(t)
-    import torch
-    torch.cuda.synchronize()
+    if torch.cuda.is_available():
+        torch.cuda.synchronize()
 
 
 def reference_sample_problem(workload):
