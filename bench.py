@@ -180,6 +180,17 @@ def reference_sample_problem(workload):
     return ms, eta_loguniform_qp(ms, seed=1), M.bc_mask_freeslip(*ms.dims), f"a {mx}x{my}x16 slab"
 
 
+def cpu_model():
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return None
+
+
 def cpu_reference_sample(workload="c2", seconds=12.0, kind="avx", ops=False):
     """Time the reference's own A11 (oracle/_ref, all host cores) on the
     workload's CPU sample; with ops=True also its diag, B and B^T."""
@@ -202,15 +213,22 @@ def cpu_reference_sample(workload="c2", seconds=12.0, kind="avx", ops=False):
             times.append(time.perf_counter() - t0)
         return min(times), len(times)
 
+    nthreads = r.set_threads(os.cpu_count())
     best, nrep = best_of(lambda: r.a11(m.dims, m.coords, eta, x, kind), seconds)
+    # one thread as well: the reference's element loop scatters under `omp critical`
+    r.set_threads(1)
+    best1, nrep1 = best_of(lambda: r.a11(m.dims, m.coords, eta, x, kind), max(1.0, seconds / 4))
+    r.set_threads(nthreads)
     out = {
         "value": m.nvel / best / 1e9,
         "unit": UNIT,
-        "cores": os.cpu_count(),
+        "cores": nthreads,
         "kind": "reference",
-        "sample": f"reference {kind} A11 (MFStokesWrapper_A11_AVX, OpenMP {os.cpu_count()} threads) on "
+        "sample": f"reference {kind} A11 (MFStokesWrapper_A11_AVX, OpenMP {nthreads} threads) on "
                   f"{what}, best of {nrep} applies",
         "seconds_per_apply": best,
+        "one_thread": {"value": m.nvel / best1 / 1e9, "seconds_per_apply": best1, "applies": nrep1},
+        "cpu_model": cpu_model(),
     }
     if ops:
         budget = max(1.0, seconds / 4)

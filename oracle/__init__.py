@@ -203,10 +203,16 @@ class RefCPU:
         L.ref_stokes_a.argtypes = [i, i, i, i, _dp, _dp, _dp, _dp, _dp, _dp]
         L.ref_marker_project.argtypes = [i, i, i, i, ctypes.POINTER(ctypes.c_int), _dp, _dp, _dp, _dp, _dp]
         L.ref_has_avx.restype = i
+        L.ref_set_threads.argtypes = [i]
+        L.ref_set_threads.restype = i
 
     @staticmethod
     def available() -> bool:
         return os.path.exists(_REF_SO)
+
+    def set_threads(self, n: int) -> int:
+        """OpenMP threads of the reference's operators; returns the count in effect."""
+        return int(self.lib.ref_set_threads(int(n)))
 
     def _check(self, rc, what):
         if rc != 0:

@@ -429,3 +429,19 @@ int ref_has_avx(void)
   return 0;
 #endif
 }
+
+/* OpenMP threads of the reference's CPU operators (the timed baseline reports
+ * all host threads and one thread); returns the count now in effect. */
+#if defined(_OPENMP)
+#include <omp.h>
+#endif
+int ref_set_threads(int n)
+{
+#if defined(_OPENMP)
+  if (n > 0) omp_set_num_threads(n);
+  return omp_get_max_threads();
+#else
+  (void)n;
+  return 1;
+#endif
+}
