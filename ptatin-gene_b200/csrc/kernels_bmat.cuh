@@ -1,0 +1,130 @@
+// Stored divergence blocks for B u (A21) and B^T p (A12) on one-rank boxes.
+//
+// Per element, B_e is the 4 x 81 block of the discrete divergence,
+//     B_e[i][3n+l] = -sum_q w_q det J_q Np_i(q) dN_n/dx_l(q)
+//                  = -sum_q w_q Np_i(q) (adj(J_q) grad_xi N_n)_l,
+// with the P1GRel pressure basis Np = {1, x^, y^, z^} of
+// P3D_ConstructNi_P1GRel_3D (src/element_utils_q2.c:183-224): the element
+// operator of MatMultMF_Stokes_MixedFEM3d_A21 / _A12
+// (src/stokes_q2p1_mf_operators_def.c:423-538).  Row i is the B^T element
+// operator of a12_colour_kernel applied to the unit pressure vector e_i,
+// stored row-major [e][i][j], 2.6 KB per element in FP64; it depends on the
+// coordinates only.
+//
+// B u is then a 4 x 81 GEMV per element (one warp, lanes over the columns, a
+// fixed-order warp reduction; no scatter: the pressure dofs are element-local)
+// and B^T p an 81 x 4 GEMV per element into per-element outputs summed per
+// node by ebe_gather_kernel in a fixed order -- both deterministic, both a
+// stream over B_e instead of a recomputation of the geometry per apply.
+#pragma once
+
+#include <cstdint>
+
+#include "kernels_colour.cuh"
+#include "q2_core.cuh"
+
+namespace ptk {
+
+constexpr int BMAT_LD = 324;  // 4 x 81 per element
+
+__global__ void __launch_bounds__(128) bmat_kernel(Box bx, const double *__restrict__ coords, double *__restrict__ Be)
+{
+  const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= (int64_t)bx.mx * bx.my * bx.mz) return;
+  const int ei = (int)(e % bx.mx), ej = (int)((e / bx.mx) % bx.my), ek = (int)(e / ((int64_t)bx.mx * bx.my));
+  int64_t nid[27];
+  element_nodes(bx, ei, ej, ek, nid);
+  double Jg[3][3][27], Xq[3][27];
+  element_jacobian(coords, nid, Jg, Xq);
+  double mean[3], invL[3];
+  p1grel_frame(coords, nid, mean, invL);
+  // per Gauss point: Jg[k][l][q] <- -w adj[l][k];  Xq[d][q] <- (x_d(q) - mean_d) / L_d
+#pragma unroll 1
+  for (int q = 0; q < 27; q++) {
+    double J[3][3], adj[3][3];
+#pragma unroll
+    for (int k = 0; k < 3; k++)
+#pragma unroll
+      for (int l = 0; l < 3; l++) J[k][l] = Jg[k][l][q];
+    (void)q2::adjugate(J, adj);
+    const double s = -q2::weight(q);
+#pragma unroll
+    for (int k = 0; k < 3; k++)
+#pragma unroll
+      for (int l = 0; l < 3; l++) Jg[k][l][q] = s * adj[l][k];
+#pragma unroll
+    for (int d = 0; d < 3; d++) Xq[d][q] = (Xq[d][q] - mean[d]) * invL[d];
+  }
+  double *out = Be + e * BMAT_LD;
+#pragma unroll 1
+  for (int i = 0; i < 4; i++)
+#pragma unroll 1
+    for (int l = 0; l < 3; l++) {
+      double dv[3][27], r[27], f[27];
+#pragma unroll
+      for (int k = 0; k < 3; k++)
+#pragma unroll
+        for (int q = 0; q < 27; q++) dv[k][q] = i == 0 ? Jg[k][l][q] : Jg[k][l][q] * Xq[i - 1][q];
+      q2::grad_colloc_t(dv[0], dv[1], dv[2], r);
+      q2::interp_t(r, f);
+#pragma unroll
+      for (int n = 0; n < 27; n++) out[i * 81 + 3 * n + l] = f[n];
+    }
+}
+
+// yp[4e+i] = sum_j B_e[i][j] u_j (MASKED: Dirichlet entries of u taken as 0).
+// One warp per element; lane sums over j = lane, lane+32, lane+64, then a
+// fixed xor-tree reduction.
+template <bool MASKED>
+__global__ void __launch_bounds__(128) bmat_a21_kernel(Box bx, const double *__restrict__ Be,
+                                                       const double *__restrict__ u,
+                                                       const uint8_t *__restrict__ mask, double *__restrict__ yp)
+{
+  const int64_t e = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (e >= (int64_t)bx.mx * bx.my * bx.mz) return;  // whole warp
+  const int ei = (int)(e % bx.mx), ej = (int)((e / bx.mx) % bx.my), ek = (int)(e / ((int64_t)bx.mx * bx.my));
+  const int64_t node0 = bx.off + 2 * (int64_t)ei + 2 * (int64_t)ej * bx.X + 2 * (int64_t)ek * bx.XY;
+  const double *b = Be + e * BMAT_LD;
+  double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+#pragma unroll
+  for (int j = lane; j < 81; j += 32) {
+    const int n = j / 3, l = j - 3 * n;
+    const int64_t k = 3 * (node0 + (n % 3) + ((n / 3) % 3) * bx.X + (n / 9) * bx.XY) + l;
+    double v = u[k];
+    if (MASKED && mask[k]) v = 0.0;
+    a0 = fma(b[j], v, a0);
+    a1 = fma(b[81 + j], v, a1);
+    a2 = fma(b[162 + j], v, a2);
+    a3 = fma(b[243 + j], v, a3);
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    a0 += __shfl_xor_sync(0xffffffffu, a0, o);
+    a1 += __shfl_xor_sync(0xffffffffu, a1, o);
+    a2 += __shfl_xor_sync(0xffffffffu, a2, o);
+    a3 += __shfl_xor_sync(0xffffffffu, a3, o);
+  }
+  if (lane == 0) {
+    double *y = yp + 4 * e;
+    y[0] = a0;
+    y[1] = a1;
+    y[2] = a2;
+    y[3] = a3;
+  }
+}
+
+// ye[e][j] = sum_i B_e[i][j] p[4e+i]: one thread per element dof.
+__global__ void bmat_a12_kernel(int64_t nel, const double *__restrict__ Be, const double *__restrict__ p,
+                                double *__restrict__ ye)
+{
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < 81 * nel; t += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t e = t / 81;
+    const int j = (int)(t - 81 * e);
+    const double *b = Be + e * BMAT_LD + j;
+    const double *pe = p + 4 * e;
+    ye[t] = fma(b[243], pe[3], fma(b[162], pe[2], fma(b[81], pe[1], b[0] * pe[0])));
+  }
+}
+
+}  // namespace ptk

@@ -309,47 +309,4 @@ __global__ void __launch_bounds__(128) a12_colour_kernel(ColourGrid g, const dou
   }
 }
 
-// A12 element contributions without a scatter: ye[e][3n+l] (one thread per
-// element, all elements in one launch); a node gather sums them in a fixed
-// order.  Used on small one-rank boxes, where the 8 colour launches of
-// a12_colour_kernel are a latency chain.
-__global__ void __launch_bounds__(128) a12_elem_kernel(Box bx, const double *__restrict__ coords,
-                                                       const double *__restrict__ p, double *__restrict__ ye)
-{
-  const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (e >= (int64_t)bx.mx * bx.my * bx.mz) return;
-  const int ei = (int)(e % bx.mx), ej = (int)((e / bx.mx) % bx.my), ek = (int)(e / ((int64_t)bx.mx * bx.my));
-  int64_t nid[27];
-  element_nodes(bx, ei, ej, ek, nid);
-  double Jg[3][3][27], Xq[3][27];
-  element_jacobian(coords, nid, Jg, Xq);
-  double mean[3], invL[3];
-  p1grel_frame(coords, nid, mean, invL);
-  const double p0 = p[4 * e], p1 = p[4 * e + 1], p2 = p[4 * e + 2], p3 = p[4 * e + 3];
-#pragma unroll 1
-  for (int q = 0; q < 27; q++) {
-    double J[3][3], adj[3][3];
-#pragma unroll
-    for (int k = 0; k < 3; k++)
-#pragma unroll
-      for (int l = 0; l < 3; l++) J[k][l] = Jg[k][l][q];
-    (void)q2::adjugate(J, adj);
-    const double pq = p0 + p1 * ((Xq[0][q] - mean[0]) * invL[0]) + p2 * ((Xq[1][q] - mean[1]) * invL[1]) +
-                      p3 * ((Xq[2][q] - mean[2]) * invL[2]);
-    const double s = -q2::weight(q) * pq;
-#pragma unroll
-    for (int k = 0; k < 3; k++)
-#pragma unroll
-      for (int l = 0; l < 3; l++) Jg[k][l][q] = s * adj[l][k];
-  }
-#pragma unroll 1
-  for (int l = 0; l < 3; l++) {
-    double r[27], f[27];
-    q2::grad_colloc_t(Jg[0][l], Jg[1][l], Jg[2][l], r);
-    q2::interp_t(r, f);
-#pragma unroll
-    for (int n = 0; n < 27; n++) ye[e * 81 + 3 * n + l] = f[n];
-  }
-}
-
 }  // namespace ptk

@@ -25,6 +25,7 @@
 #include "kernels_tmem.cuh"
 #include "kernels_ebe.cuh"
 #include "kernels_markers.cuh"
+#include "kernels_bmat.cuh"
 #include "kernels_galerkin.cuh"
 
 #include <cub/device/device_radix_sort.cuh>
@@ -89,6 +90,8 @@ struct pt_op {
   int64_t MXP;
   int TX, ntx, LZ, nzc;
   bool geom_dirty, geom_ok, full_box, ebe_valid;
+  bool be_valid;  // d_Be matches the coordinates
+  double *d_Be;   // divergence blocks [nel][4][81] (one-rank boxes, built on first B / B^T use)
   int a11_kernel;
   int64_t launches;
   uint64_t state;  // bumped whenever coordinates, viscosity or the mask change
@@ -453,8 +456,29 @@ pt_status diag_d(pt_op *op, double *d)
   return PT_OK;
 }
 
+// Divergence blocks of the current coordinates (one-rank boxes), built on first use.
+pt_status ensure_be(pt_op *op)
+{
+  if (op->be_valid) return PT_OK;
+  if (!op->d_Be) PT_CUDA(op_alloc(op, (void **)&op->d_Be, sizeof(double) * ptk::BMAT_LD * op->nel));
+  ptk::bmat_kernel<<<nblocks(op->nel), TPB, 0, op->stream>>>(op->box, op->d_coords, op->d_Be);
+  PT_LAUNCHED(op);
+  op->be_valid = true;
+  return PT_OK;
+}
+
 pt_status a21_d(pt_op *op, const double *u, double *yp, bool masked)
 {
+  if (op->full_box) {
+    pt_status s = ensure_be(op);
+    if (s != PT_OK) return s;
+    if (masked)
+      ptk::bmat_a21_kernel<true><<<nblocks(32 * op->nel), TPB, 0, op->stream>>>(op->box, op->d_Be, u, op->d_mask, yp);
+    else
+      ptk::bmat_a21_kernel<false><<<nblocks(32 * op->nel), TPB, 0, op->stream>>>(op->box, op->d_Be, u, nullptr, yp);
+    PT_LAUNCHED(op);
+    return PT_OK;
+  }
   if (masked)
     ptk::a21_kernel<true><<<nblocks(op->nel), TPB, 0, op->stream>>>(op->box, op->d_coords, u, op->d_mask, yp);
   else
@@ -466,10 +490,12 @@ pt_status a21_d(pt_op *op, const double *u, double *yp, bool masked)
 // yu = B^T p, or yu += B^T p (accumulate)
 pt_status a12_d(pt_op *op, const double *p, double *yu, bool accumulate = false)
 {
-  if (op->a11_kernel == A11_EBE && op->full_box) {
-    // small box: element contributions in one launch, then the node gather
+  if (op->full_box) {
+    // one-rank box: element contributions from the stored blocks, then the node gather
+    pt_status s = ensure_be(op);
+    if (s != PT_OK) return s;
     if (!op->d_ye) PT_CUDA(op_alloc(op, (void **)&op->d_ye, sizeof(double) * 81 * op->nel));
-    ptk::a12_elem_kernel<<<nblocks(op->nel), TPB, 0, op->stream>>>(op->box, op->d_coords, p, op->d_ye);
+    ptk::bmat_a12_kernel<<<grid_stride_blocks(81 * op->nel), 256, 0, op->stream>>>(op->nel, op->d_Be, p, op->d_ye);
     PT_LAUNCHED(op);
     if (accumulate)
       ptk::ebe_gather_kernel<double, false, true><<<grid_stride_blocks(op->nvel), 256, 0, op->stream>>>(
@@ -689,7 +715,7 @@ pt_status pt_op_destroy(pt_op *op)
   if (op->stream && !op->pool) cudaStreamSynchronize(op->stream);
   void *bufs[] = {op->d_coords, op->d_eta, op->d_coords32, op->d_eta32, op->d_mask, op->d_u,
                   op->d_y, op->d_p, op->d_K, op->d_K32, op->d_bad, op->d_Ae, op->d_Ae32, op->d_ye,
-                  op->mk_scratch};
+                  op->mk_scratch, op->d_Be};
   for (void *b : bufs) op_free(op, b);
   if (op->own_stream && op->stream) cudaStreamDestroy(op->stream);
   if (op->pipe_ready) {
@@ -731,6 +757,7 @@ static pt_status finish_coords(pt_op *op)
   PT_LAUNCHED(op);
   op->has_coords = true;
   op->geom_dirty = true;
+  op->be_valid = false;
   op->state++;
   return PT_OK;
 }
