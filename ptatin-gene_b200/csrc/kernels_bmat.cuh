@@ -13,8 +13,8 @@
 //
 // B u is then a 4 x 81 GEMV per element (one warp, lanes over the columns, a
 // fixed-order warp reduction; no scatter: the pressure dofs are element-local)
-// and B^T p an 81 x 4 GEMV per element into per-element outputs summed per
-// node by ebe_gather_kernel in a fixed order -- both deterministic, both a
+// and B^T p a node-centred sum over the (<= 8) elements of each node of their
+// 4-term column products, in a fixed order -- both deterministic, both a
 // stream over B_e instead of a recomputation of the geometry per apply.
 #pragma once
 
@@ -114,16 +114,45 @@ __global__ void __launch_bounds__(128) bmat_a21_kernel(Box bx, const double *__r
   }
 }
 
-// ye[e][j] = sum_i B_e[i][j] p[4e+i]: one thread per element dof.
-__global__ void bmat_a12_kernel(int64_t nel, const double *__restrict__ Be, const double *__restrict__ p,
-                                double *__restrict__ ye)
+// B^T p node by node: y_k = sum over the (<= 8) elements of node k, in the
+// order of ebe_gather_kernel, of sum_i B_e[i][j] p[4e+i] (j = the node's dof in
+// element e), with no per-element output array (ACC: added to y).
+// One-rank boxes (node box = element box).
+template <bool ACC>
+__global__ void bmat_a12_gather_kernel(Box b, const double *__restrict__ Be, const double *__restrict__ p,
+                                       double *__restrict__ y)
 {
-  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < 81 * nel; t += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t e = t / 81;
-    const int j = (int)(t - 81 * e);
-    const double *b = Be + e * BMAT_LD + j;
-    const double *pe = p + 4 * e;
-    ye[t] = fma(b[243], pe[3], fma(b[162], pe[2], fma(b[81], pe[1], b[0] * pe[0])));
+  const int64_t n = 3 * b.XY * (2 * (int64_t)b.mz + 1);
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) {
+    const int l = (int)(t % 3);
+    const int64_t node = t / 3;
+    const int i = (int)(node % b.X), j = (int)((node / b.X) % (2 * b.my + 1)), k = (int)(node / b.XY);
+    int ex[2], lx[2], nx = 0, ey[2], ly[2], ny = 0, ez[2], lz[2], nz = 0;
+    if (i & 1) { ex[0] = i >> 1; lx[0] = 1; nx = 1; }
+    else {
+      if (i > 0) { ex[nx] = (i >> 1) - 1; lx[nx++] = 2; }
+      if ((i >> 1) < b.mx) { ex[nx] = i >> 1; lx[nx++] = 0; }
+    }
+    if (j & 1) { ey[0] = j >> 1; ly[0] = 1; ny = 1; }
+    else {
+      if (j > 0) { ey[ny] = (j >> 1) - 1; ly[ny++] = 2; }
+      if ((j >> 1) < b.my) { ey[ny] = j >> 1; ly[ny++] = 0; }
+    }
+    if (k & 1) { ez[0] = k >> 1; lz[0] = 1; nz = 1; }
+    else {
+      if (k > 0) { ez[nz] = (k >> 1) - 1; lz[nz++] = 2; }
+      if ((k >> 1) < b.mz) { ez[nz] = k >> 1; lz[nz++] = 0; }
+    }
+    double acc = 0.0;
+    for (int c = 0; c < nz; c++)
+      for (int bb = 0; bb < ny; bb++)
+        for (int a = 0; a < nx; a++) {
+          const int64_t e = ex[a] + (int64_t)b.mx * (ey[bb] + (int64_t)b.my * ez[c]);
+          const double *be = Be + e * BMAT_LD + 3 * (lx[a] + 3 * ly[bb] + 9 * lz[c]) + l;
+          const double *pe = p + 4 * e;
+          acc += fma(be[243], pe[3], fma(be[162], pe[2], fma(be[81], pe[1], be[0] * pe[0])));
+        }
+    y[t] = ACC ? y[t] + acc : acc;
   }
 }
 

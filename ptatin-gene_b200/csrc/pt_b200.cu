@@ -491,18 +491,13 @@ pt_status a21_d(pt_op *op, const double *u, double *yp, bool masked)
 pt_status a12_d(pt_op *op, const double *p, double *yu, bool accumulate = false)
 {
   if (op->full_box) {
-    // one-rank box: element contributions from the stored blocks, then the node gather
+    // one-rank box: node by node from the stored blocks
     pt_status s = ensure_be(op);
     if (s != PT_OK) return s;
-    if (!op->d_ye) PT_CUDA(op_alloc(op, (void **)&op->d_ye, sizeof(double) * 81 * op->nel));
-    ptk::bmat_a12_kernel<<<grid_stride_blocks(81 * op->nel), 256, 0, op->stream>>>(op->nel, op->d_Be, p, op->d_ye);
-    PT_LAUNCHED(op);
     if (accumulate)
-      ptk::ebe_gather_kernel<double, false, true><<<grid_stride_blocks(op->nvel), 256, 0, op->stream>>>(
-          op->box, op->d_ye, nullptr, nullptr, yu);
+      ptk::bmat_a12_gather_kernel<true><<<grid_stride_blocks(op->nvel), 256, 0, op->stream>>>(op->box, op->d_Be, p, yu);
     else
-      ptk::ebe_gather_kernel<double, false><<<grid_stride_blocks(op->nvel), 256, 0, op->stream>>>(
-          op->box, op->d_ye, nullptr, nullptr, yu);
+      ptk::bmat_a12_gather_kernel<false><<<grid_stride_blocks(op->nvel), 256, 0, op->stream>>>(op->box, op->d_Be, p, yu);
     PT_LAUNCHED(op);
     return PT_OK;
   }
