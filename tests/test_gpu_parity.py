@@ -331,3 +331,23 @@ def test_marker_projection_rejects_markers_outside_the_box(torch_cuda):
         wil[11] = 1 << 30
         with pytest.raises(PtError, match="3 markers have an element index outside"):
             op.ProjectMarkers(wil, xi, e, r, install=False)
+
+
+def test_divergence_blocks_follow_coordinate_updates(torch_cuda, ora):
+    """B u and B^T p use element blocks stored from the coordinates: after new
+    coordinates they are rebuilt (a viscosity update keeps them), so both
+    applies still match the oracle on the new mesh."""
+    from pt_b200 import MatStokesMF
+    m, eta, mask = M.problem("box:6,5,4", seed=8)
+    m2 = M.make_mesh(*m.dims, perturb=0.1, seed=99)
+    x = M.uniform_vec(m.nvel, 3)
+    p = M.uniform_vec(m.npres, 4)
+    with MatStokesMF(*m.dims) as op:
+        op.SetUp(m.coords, eta, mask)
+        assert relerr(op.MFStokesWrapper_A21(x), ora.a21(m.dims, m.coords, x)) < TOL64
+        op.set_eta(eta[::-1].copy())
+        assert relerr(op.MFStokesWrapper_A12(p), ora.a12(m.dims, m.coords, p)) < TOL64
+        op.set_coords(m2.coords)
+        assert relerr(op.MFStokesWrapper_A21(x), ora.a21(m.dims, m2.coords, x)) < TOL64
+        assert relerr(op.MFStokesWrapper_A12(p), ora.a12(m.dims, m2.coords, p)) < TOL64
+        assert relerr(op.MatMult_MFStokes_A12(p), ora.matmult_a12(m.dims, m2.coords, mask, p)) < TOL64
