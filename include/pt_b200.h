@@ -348,7 +348,7 @@ pt_status pt_project_markers_h(pt_op *op, int64_t n, const int32_t *wil, const d
 
 /* Select the A11 kernel by name, like the reference's -a11_op function list
  * (src/stokes_operators.c:123-154).  Names: "b200" (default: stored element
- * matrices for one-rank boxes of at most 4096 elements, the streaming kernel
+ * matrices for one-rank boxes of at most 32768 elements, the streaming kernel
  * above), "b200_stream" (the streaming kernel with precomputed Gauss-point
  * geometry), "b200_ebe" (stored 81x81 element matrices, element GEMV + node
  * gather; one-rank boxes), "b200_tmem" (the streaming kernel with TMEM

@@ -65,10 +65,11 @@ pt_status fail(pt_status s, const char *fmt, ...)
 enum A11Kernel { A11_STREAM = 0, A11_COLOUR = 1, A11_TMEM = 2, A11_EBE = 3 };
 
 // "b200" picks stored element matrices for one-rank boxes up to this many
-// elements (FP64 + FP32 matrices: 78 KB per element) and the streaming kernel
-// above.  Measured at 8^3: 2 launches vs a 0.2 ms latency chain of 4 colour
-// launches.
-constexpr int64_t EBE_AUTO_MAX_ELEMENTS = 4096;
+// elements (packed FP64 + FP32 matrices: 40 KB per element, 1.3 GB at 32^3)
+// and the streaming kernel above.  Measured FP64 / FP32 apply, stored
+// matrices vs streaming: 16^3 0.037 / 0.023 vs 0.26 / 0.22 ms, 32^3 0.24 /
+// 0.14 vs 0.35 / 0.30 ms, 40^3 0.45 / 0.27 vs 0.36 / 0.27 ms.
+constexpr int64_t EBE_AUTO_MAX_ELEMENTS = 32768;
 
 }  // namespace
 

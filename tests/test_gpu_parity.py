@@ -174,7 +174,7 @@ def test_tiling_schedules_agree_with_the_oracle(ora):
     m, eta, mask = M.problem("box:40,9,13", seed=21)
     x = M.uniform_vec(m.nvel, 22)
     ref = ora.matmult_a11(m.dims, m.coords, eta, mask, x)
-    with MatStokesMF(*m.dims) as op:
+    with MatStokesMF(*m.dims, a11_op="b200_stream") as op:
         op.SetUp(m.coords, eta, mask)
         default = op.tiling
         xd = torch.from_numpy(x).cuda()
@@ -199,7 +199,7 @@ def test_pipelined_host_apply_is_bitwise_the_device_apply(lz):
     from pt_b200 import MatStokesMF
     m, eta, mask = M.problem("box:24,10,30", seed=23)
     x = M.uniform_vec(m.nvel, 24)
-    with MatStokesMF(*m.dims) as op:
+    with MatStokesMF(*m.dims, a11_op="b200_stream") as op:
         op.SetUp(m.coords, eta, mask)
         op.set_tiling(lz)
         xd = torch.from_numpy(x).cuda()
