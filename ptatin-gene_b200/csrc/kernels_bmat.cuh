@@ -8,8 +8,8 @@
 // operator of MatMultMF_Stokes_MixedFEM3d_A21 / _A12
 // (src/stokes_q2p1_mf_operators_def.c:423-538).  Row i is the B^T element
 // operator of a12_colour_kernel applied to the unit pressure vector e_i,
-// stored row-major [e][i][j], 2.6 KB per element in FP64; it depends on the
-// coordinates only.
+// stored column-major [e][j][i] (a column's four entries are one 32-byte
+// sector), 2.6 KB per element in FP64; it depends on the coordinates only.
 //
 // B u is then a 4 x 81 GEMV per element (one warp, lanes over the columns, a
 // fixed-order warp reduction; no scatter: the pressure dofs are element-local)
@@ -68,13 +68,15 @@ __global__ void __launch_bounds__(128) bmat_kernel(Box bx, const double *__restr
       q2::grad_colloc_t(dv[0], dv[1], dv[2], r);
       q2::interp_t(r, f);
 #pragma unroll
-      for (int n = 0; n < 27; n++) out[i * 81 + 3 * n + l] = f[n];
+      for (int n = 0; n < 27; n++) out[(3 * n + l) * 4 + i] = f[n];
     }
 }
 
 // yp[4e+i] = sum_j B_e[i][j] u_j (MASKED: Dirichlet entries of u taken as 0).
-// One warp per element; lane sums over j = lane, lane+32, lane+64, then a
-// fixed xor-tree reduction.
+// One warp per element.  The block is read as 162 16-byte pairs (B_e[j][0..1]
+// or B_e[j][2..3]), 32 consecutive pairs per warp load: even lanes sum rows 0
+// and 1, odd lanes rows 2 and 3, then a fixed xor-tree reduction over the
+// lanes of each parity.
 template <bool MASKED>
 __global__ void __launch_bounds__(128) bmat_a21_kernel(Box bx, const double *__restrict__ Be,
                                                        const double *__restrict__ u,
@@ -85,32 +87,30 @@ __global__ void __launch_bounds__(128) bmat_a21_kernel(Box bx, const double *__r
   if (e >= (int64_t)bx.mx * bx.my * bx.mz) return;  // whole warp
   const int ei = (int)(e % bx.mx), ej = (int)((e / bx.mx) % bx.my), ek = (int)(e / ((int64_t)bx.mx * bx.my));
   const int64_t node0 = bx.off + 2 * (int64_t)ei + 2 * (int64_t)ej * bx.X + 2 * (int64_t)ek * bx.XY;
-  const double *b = Be + e * BMAT_LD;
-  double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+  const double2 *b2 = reinterpret_cast<const double2 *>(Be + e * BMAT_LD);
+  double s0 = 0.0, s1 = 0.0;
 #pragma unroll
-  for (int j = lane; j < 81; j += 32) {
-    const int n = j / 3, l = j - 3 * n;
-    const int64_t k = 3 * (node0 + (n % 3) + ((n / 3) % 3) * bx.X + (n / 9) * bx.XY) + l;
-    double v = u[k];
-    if (MASKED && mask[k]) v = 0.0;
-    a0 = fma(b[j], v, a0);
-    a1 = fma(b[81 + j], v, a1);
-    a2 = fma(b[162 + j], v, a2);
-    a3 = fma(b[243 + j], v, a3);
+  for (int it = 0; it < 6; it++) {
+    const int idx = lane + 32 * it;
+    if (idx < 162) {
+      const int j = idx >> 1, n = j / 3, l = j - 3 * n;
+      const int64_t k = 3 * (node0 + (n % 3) + ((n / 3) % 3) * bx.X + (n / 9) * bx.XY) + l;
+      double v = u[k];
+      if (MASKED && mask[k]) v = 0.0;
+      const double2 c = b2[idx];
+      s0 = fma(c.x, v, s0);
+      s1 = fma(c.y, v, s1);
+    }
   }
 #pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    a0 += __shfl_xor_sync(0xffffffffu, a0, o);
-    a1 += __shfl_xor_sync(0xffffffffu, a1, o);
-    a2 += __shfl_xor_sync(0xffffffffu, a2, o);
-    a3 += __shfl_xor_sync(0xffffffffu, a3, o);
+  for (int o = 16; o > 1; o >>= 1) {
+    s0 += __shfl_xor_sync(0xffffffffu, s0, o);
+    s1 += __shfl_xor_sync(0xffffffffu, s1, o);
   }
-  if (lane == 0) {
-    double *y = yp + 4 * e;
-    y[0] = a0;
-    y[1] = a1;
-    y[2] = a2;
-    y[3] = a3;
+  if (lane < 2) {
+    double *y = yp + 4 * e + 2 * lane;
+    y[0] = s0;
+    y[1] = s1;
   }
 }
 
@@ -148,9 +148,11 @@ __global__ void bmat_a12_gather_kernel(Box b, const double *__restrict__ Be, con
       for (int bb = 0; bb < ny; bb++)
         for (int a = 0; a < nx; a++) {
           const int64_t e = ex[a] + (int64_t)b.mx * (ey[bb] + (int64_t)b.my * ez[c]);
-          const double *be = Be + e * BMAT_LD + 3 * (lx[a] + 3 * ly[bb] + 9 * lz[c]) + l;
+          const double *be = Be + e * BMAT_LD + 4 * (3 * (lx[a] + 3 * ly[bb] + 9 * lz[c]) + l);
+          const double2 c01 = *reinterpret_cast<const double2 *>(be);
+          const double2 c23 = *reinterpret_cast<const double2 *>(be + 2);
           const double *pe = p + 4 * e;
-          acc += fma(be[243], pe[3], fma(be[162], pe[2], fma(be[81], pe[1], be[0] * pe[0])));
+          acc += fma(c23.y, pe[3], fma(c23.x, pe[2], fma(c01.y, pe[1], c01.x * pe[0])));
         }
     y[t] = ACC ? y[t] + acc : acc;
   }
