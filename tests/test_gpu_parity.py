@@ -230,16 +230,18 @@ def test_stokes_operator_matches_reference(torch_cuda, name, a11_op):
             assert relerr(yp, g["a_p_" + kind]) < TOL64
 
 
-@pytest.mark.parametrize("workload", ["c0", "box:3,2,4", "box:7,5,3", "box:65,9,7", "box:40,20,9"])
-def test_matmult_stokes_a_matches_oracle(torch_cuda, ora, workload):
+@pytest.mark.parametrize("workload", ["c0", "box:3,2,4", "box:7,5,3", "box:65,9,7", "box:40,20,9", "box:130,3,4"])
+@pytest.mark.parametrize("a11_op", ["b200", "b200_stream"])
+def test_matmult_stokes_a_matches_oracle(torch_cuda, ora, workload, a11_op):
     """MatMult_MFStokes_A on one rank (device and host paths) against the
-    oracle's restatement of its BC semantics."""
+    oracle's restatement of its BC semantics, with the default op (stored
+    element matrices on these small boxes) and with the streaming kernel."""
     torch = torch_cuda
     m, eta, mask = M.problem(workload, seed=31)
     u = M.uniform_vec(m.nvel, 32)
     p = M.uniform_vec(m.npres, 33)
     ru, rp = ora.matmult_a(m.dims, m.coords, eta, mask, u, p)
-    with make_op(m, eta, mask) as op:
+    with make_op(m, eta, mask, a11_op) as op:
         yu, yp = op.MatMult_MFStokes_A(u, p)
         assert relerr(yu, ru) < TOL64 and relerr(yp, rp) < TOL64
         du, dp = op.MatMult_MFStokes_A(torch.from_numpy(u).cuda(), torch.from_numpy(p).cuda())
