@@ -552,7 +552,7 @@ pt_status mg_level_setup(pt_solver *s, pt_mg &mg, pt_mg_level &L, const pt_op *n
   return PT_OK;
 }
 
-constexpr int64_t MG_GALERKIN_MAX_ELEMENTS = 262144;  // Galerkin levels up to 64^3 elements (13.8 GB FP64)
+constexpr int64_t MG_GALERKIN_MAX_ELEMENTS = 262144;  // Galerkin levels up to 64^3 elements (7.0 GB FP64, packed)
 
 // Galerkin coarse operators (mg_assembled = 2): every level from the first
 // one of <= MG_GALERKIN_MAX_ELEMENTS elements down gets element matrices
