@@ -420,8 +420,10 @@ def run_solve(args):
     fd = torch.from_numpy(f).cuda()
     op = MatStokesMF(*m.dims)
     op.SetUp(m.coords, eta, mask)
+    # the fine level's tile schedule from the autotuner, as in the apply bench
+    lz, _ = op.autotune_tiling(fd) if not args.no_autotune else (op.tiling, None)
     out = {"mode": "solve", "workload": args.workload, "nvel": m.nvel, "ksp": args.ksp, "pc": args.pc,
-           "cheby_degree": args.cheby_degree, "rtol": args.rtol}
+           "cheby_degree": args.cheby_degree, "rtol": args.rtol, "tiling_lz": lz}
     sols = {}
     for name, fp32 in (("fp64", 0), ("fp32_smoothed", 1)):
         x = torch.zeros_like(fd)
