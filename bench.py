@@ -18,8 +18,15 @@ e2e       = the same metric through the public host-pointer API
 roofline  = algorithmic bytes of one apply / its device time against the
             measured HBM copy bandwidth (MEASURED_PEAKS.json).
 cpu_baseline = the reference's own AVX A11 (oracle/_ref, compiled from the
-            reference sources) on a 128x128x16 slab of the same workload,
-            on all host cores.
+            reference sources) on the same 128^3 box and inputs, on all host
+            cores; the same leg runs the reference's diag, B, B^T and whole
+            Stokes operator once and checks every device output of the line
+            against them (parity: max-norm relative error).
+extra     = FP32 A11, diag, B, B^T and whole-operator rates, and the rest of
+            the metric: the precision-form solve (FP64- vs FP32-smoothed
+            flexible CG to rtol 1e-8 on this box, true residual from the
+            reference's A11 on the host), the batched form (256 boxes) and a
+            served stream (p50/p99, solves/s against serial plain solves).
 --impl reference times that reference CPU path only and prints its line.
 """
 from __future__ import annotations
@@ -163,21 +170,12 @@ def barrier(pg, device):
         torch.cuda.synchronize()
 
 
-def reference_sample_problem(workload):
-    """The CPU sample of a workload: the whole problem when it has at most
-    300k elements, else a 16-layer z-slab of it (same generators)."""
+def reference_problem(workload):
+    """The workload the reference CPU path runs: the same box, viscosity and
+    BCs as the device leg (the whole problem, every size)."""
     from pt_b200 import mesh as M
-    m, eta, mask = M.problem(workload, seed=0) if workload != "c2" else (None, None, None)
-    if m is not None and m.nel <= 300_000:
-        return m, eta, mask, f"the whole {m.mx}x{m.my}x{m.mz} problem"
-    if m is None or workload == "c2":
-        m = M.make_mesh(128, 128, 16, perturb=0.05, seed=0)
-        eta = M.eta_layered(m, seed=1)
-        return m, eta, M.bc_mask_freeslip(*m.dims), "a 128x128x16 slab of the 128^3 workload"
-    mx, my, mz = m.dims
-    ms = M.make_mesh(mx, my, 16, perturb=0.05, seed=0)
-    from pt_b200.mesh import eta_loguniform_qp
-    return ms, eta_loguniform_qp(ms, seed=1), M.bc_mask_freeslip(*ms.dims), f"a {mx}x{my}x16 slab"
+    m, eta, mask = M.problem(workload, seed=0)
+    return m, eta, mask, f"the whole {m.mx}x{m.my}x{m.mz} problem"
 
 
 def cpu_model():
@@ -191,56 +189,84 @@ def cpu_model():
     return None
 
 
-def cpu_reference_sample(workload="c2", seconds=12.0, kind="avx", ops=False):
-    """Time the reference's own A11 (oracle/_ref, all host cores) on the
-    workload's CPU sample; with ops=True also its diag, B and B^T."""
+def _relerr(a, b):
+    a = np.asarray(a, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
+
+
+def cpu_reference_leg(m, eta, mask, x, p, seconds=12.0, kind="avx", device_out=None):
+    """The reference's own A11 (oracle/_ref, all host cores) on the device leg's
+    box and inputs: best of the applies that fit in `seconds` (at least two),
+    one apply on one thread, and one run of its diag, B, B^T and whole Stokes
+    operator.  With device_out = {name: host array} each device result is
+    checked against the reference's (MatShell-level BC rules of
+    src/stokes_operators.c); returns (cpu_baseline dict, parity dict)."""
     import oracle
-    from pt_b200 import mesh as M
     if not oracle.RefCPU.available():
         oracle.build()
     r = oracle.RefCPU()
-    m, eta, mask, what = reference_sample_problem(workload)
-    x = M.uniform_vec(m.nvel, 7)
-    x[mask.astype(bool)] = 0.0
-    p = M.uniform_vec(m.npres, 8)
 
     def best_of(fn, budget):
-        fn()  # warm-up
+        out = fn()  # warm-up (and the output to check)
         times, t_end = [], time.perf_counter() + budget
         while time.perf_counter() < t_end or len(times) < 2:
             t0 = time.perf_counter()
             fn()
             times.append(time.perf_counter() - t0)
-        return min(times), len(times)
+        return min(times), len(times), out
+
+    def once(fn):
+        t0 = time.perf_counter()
+        out = fn()
+        return time.perf_counter() - t0, out
 
     nthreads = r.set_threads(os.cpu_count())
-    best, nrep = best_of(lambda: r.a11(m.dims, m.coords, eta, x, kind), seconds)
+    best, nrep, y_ref = best_of(lambda: r.matmult_a11(m.dims, m.coords, eta, mask, x, kind), seconds)
     # one thread as well: the reference's element loop scatters under `omp critical`
     r.set_threads(1)
-    best1, nrep1 = best_of(lambda: r.a11(m.dims, m.coords, eta, x, kind), max(1.0, seconds / 4))
+    t1, _ = once(lambda: r.matmult_a11(m.dims, m.coords, eta, mask, x, kind))
     r.set_threads(nthreads)
-    out = {
+    t_diag, d_ref = once(lambda: r.getdiag_a11(m.dims, m.coords, eta, mask))
+    t_a21, bu_ref = once(lambda: r.matmult_a21(m.dims, m.coords, mask, x))
+    t_a12, btp_ref = once(lambda: r.matmult_a12(m.dims, m.coords, mask, p, kind))
+    t_a, (au_ref, ap_ref) = once(lambda: r.matmult_a(m.dims, m.coords, eta, mask, x, p, kind))
+    secs = {"diag": t_diag, "a21": t_a21, "a12": t_a12, "stokes_a": t_a}
+    what = f"the whole {m.mx}x{m.my}x{m.mz} problem"
+    cpu = {
         "value": m.nvel / best / 1e9,
         "unit": UNIT,
         "cores": nthreads,
         "kind": "reference",
-        "sample": f"reference {kind} A11 (MFStokesWrapper_A11_AVX, OpenMP {nthreads} threads) on "
-                  f"{what}, best of {nrep} applies",
+        "sample": f"reference {kind} A11 (MatMult_MFStokes_A11 over MFStokesWrapper_A11_AVX, OpenMP {nthreads} "
+                  f"threads) on {what}, same inputs as the device leg, best of {nrep} applies",
         "seconds_per_apply": best,
-        "one_thread": {"value": m.nvel / best1 / 1e9, "seconds_per_apply": best1, "applies": nrep1},
+        "one_thread": {"value": m.nvel / t1 / 1e9, "seconds_per_apply": t1, "applies": 1},
         "cpu_model": cpu_model(),
+        "ops_seconds": secs,
+        "ops_gdofs": {k: (m.nvel + (m.npres if k == "stokes_a" else 0)) / v / 1e9 for k, v in secs.items()},
     }
-    if ops:
-        budget = max(1.0, seconds / 4)
-        out["ops_seconds"] = {
-            "diag": best_of(lambda: r.diag(m.dims, m.coords, eta), budget)[0],
-            "a21": best_of(lambda: r.a21(m.dims, m.coords, x), budget)[0],
-            "a12": best_of(lambda: r.a12(m.dims, m.coords, p, "avx"), budget)[0],
-            "stokes_a": best_of(lambda: r.stokes_a(m.dims, m.coords, eta, x, p, "avx"), budget)[0],
-        }
-        out["ops_gdofs"] = {k: (m.nvel + (m.npres if k == "stokes_a" else 0)) / v / 1e9
-                            for k, v in out["ops_seconds"].items()}
-    return out
+    parity = None
+    if device_out is not None:
+        refs = {"a11": y_ref, "diag": d_ref, "a21": bu_ref, "a12": btp_ref, "stokes_a_u": au_ref,
+                "stokes_a_p": ap_ref}
+        parity = {k: _relerr(device_out[k], v) for k, v in refs.items() if k in device_out}
+        parity["max"] = max(parity.values()) if parity else None
+        parity["against"] = (f"the reference's own CPU operators (oracle/_ref, {kind}) on {what}, "
+                             "MatShell-level BC rules, max-norm relative error")
+    return cpu, parity
+
+
+def reference_residual(m, eta, mask, f, xsol, kind="avx"):
+    """True FP64 relative residual ||f - A11 x|| / ||f|| of a device solution,
+    with the reference's own A11 on the host (all cores)."""
+    import oracle
+    if not oracle.RefCPU.available():
+        oracle.build()
+    r = oracle.RefCPU()
+    r.set_threads(os.cpu_count())
+    res = f - r.matmult_a11(m.dims, m.coords, eta, mask, xsol, kind)
+    return float(np.linalg.norm(res) / np.linalg.norm(f))
 
 
 def run_reference(args):
@@ -257,24 +283,30 @@ def run_reference(args):
         return 0
     from pt_b200 import mesh as M
     r = oracle.RefCPU()
-    m, eta, mask, what = reference_sample_problem(args.workload)
+    nthreads = r.set_threads(os.cpu_count())
+    m, eta, mask, what = reference_problem(args.workload)
     x = M.uniform_vec(m.nvel, 7)
-    x[mask.astype(bool)] = 0.0
+    # MatMult_MFStokes_A11 on the same inputs as the device leg (Dirichlet
+    # columns zeroed, rows copied) through the reference's AVX element loop
     for _ in range(args.warmup):
-        r.a11(m.dims, m.coords, eta, x, "avx")
+        r.matmult_a11(m.dims, m.coords, eta, mask, x, "avx")
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        r.a11(m.dims, m.coords, eta, x, "avx")
+        r.matmult_a11(m.dims, m.coords, eta, mask, x, "avx")
     dt = (time.perf_counter() - t0) / args.steps
     v = m.nvel / dt / 1e9
     line = {
         "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"A11 FP64 apply on {what} ({args.workload}), reference CPU (oracle/_ref, avx)",
-                   "global_batch": 1, "seq_len": 0, "parallelism": "cpu-openmp"},
-        "cpu_baseline": {"value": v, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
-                         "sample": f"{what}, MFStokesWrapper_A11_AVX compiled from the reference sources"},
+        "config": {"workload": f"A11 FP64 MatMult, {m.mx}x{m.my}x{m.mz} Q2 box ({m.nvel} velocity dofs), "
+                               f"{WORKLOAD_TEXT.get(args.workload.split(':')[0], args.workload)}, free-slip BCs",
+                   "global_batch": 1, "seq_len": 0, "parallelism": "cpu-openmp",
+                   "impl_detail": "reference CPU (oracle/_ref: MFStokesWrapper_A11_AVX compiled from the "
+                                  "reference sources)"},
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": nthreads, "kind": "reference",
+                         "sample": f"{what}, every step one MatMult_MFStokes_A11 through the reference's AVX "
+                                   "element loop compiled from its sources"},
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
@@ -329,6 +361,9 @@ def run_ours(args):
     t_apply = t / args.steps
     value = ws * m.nvel / t_apply / 1e9
 
+    # the timed apply's own output, checked against the reference below
+    y_timed = y.cpu().numpy() if rank == 0 and ws == 1 else None
+
     # ---- roofline of the A11 apply ---------------------------------------------
     peak, peak_kind = load_peaks()
     bytes_alg = algorithmic_bytes(m)
@@ -367,13 +402,34 @@ def run_ours(args):
            "d2h_bytes_per_step": 8 * m.nvel, "ms_per_step": t_e2e * 1e3,
            "path": "pt_matmult_a11_h (MatMult_MFStokes_A11 on pinned numpy arrays)"}
 
-    cpu = None
+    cpu, parity = None, None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        # device outputs of every operator on the bench inputs (host copies)
+        dout = {"a11": y_timed}
+        if not args.quick:
+            dout["diag"] = op.MatGetDiagonal_MFStokes_A11(y).cpu().numpy()
+            dout["a21"] = op.MatMult_MFStokes_A21(x, yp).cpu().numpy()
+            dout["a12"] = op.MatMult_MFStokes_A12(p, y).cpu().numpy()
+            au, ap = op.MatMult_MFStokes_A(x, p, y, yp)
+            dout["stokes_a_u"], dout["stokes_a_p"] = au.cpu().numpy(), ap.cpu().numpy()
         try:
-            cpu = cpu_reference_sample(args.workload, seconds=args.cpu_seconds, ops=not args.quick)
+            cpu, parity = cpu_reference_leg(m, eta, mask, x.cpu().numpy(), p.cpu().numpy(),
+                                            seconds=args.cpu_seconds, device_out=dout)
         except Exception as e:  # pragma: no cover
             cpu = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
                    "sample": f"unavailable: {e}"}
+        del dout
+
+    # ---- the rest of the metric: precision-form solve, batched, served ------------
+    if rank == 0 and ws == 1 and not args.quick and not args.no_legs:
+        extra["solve"] = solve_leg(op, m, eta, mask, args, check=not args.no_cpu_baseline)
+    op.Destroy()
+    del x, y, x32, y32, p, yp
+    torch.cuda.empty_cache()
+    if rank == 0 and ws == 1 and not args.quick and not args.no_legs:
+        extra["batched"] = batched_leg(args.nbatch, args.steps)
+        torch.cuda.empty_cache()
+        extra["serve"] = serve_leg(args, nreq=args.leg_nreq, ncal=args.leg_ncal, nserial=args.leg_nserial)
 
     if rank == 0:
         line = {
@@ -386,58 +442,80 @@ def run_ours(args):
                        "a11_op": op.a11_op, "tiling": tiling, "l2": "inputs larger than L2 (no flush)"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": TRAFFIC_PER_ELEMENT_F64 * m.nel,
-                         "traffic_source": "ncu dram__bytes_read+write of the 4 colour launches of one 96^3 apply "
-                                           "(profiles/a11_stream_96cubed.md), scaled by the element count",
+                         "traffic_source": "ncu dram__bytes_read+write of the 4 colour launches of one 96^3 apply, "
+                                           "scaled by the element count",
                          "peak_kind": peak_kind, "algorithmic_bytes_per_apply": bytes_alg},
             "cpu_baseline": cpu,
+            "parity_relerr": parity["max"] if parity else None,
+            "parity": parity,
             "e2e": e2e,
             "gpu_launches": launches,
             "clocks": clk.summary(),
             "extra": extra,
         }
         print(json.dumps(line))
-    op.Destroy()
     if pg is not None:
         pg.destroy_process_group()
     return 0
 
 
-def run_solve(args):
-    """Precision form: A11 u = f with f uniform [-1, 1] on free dofs, FP64
-    outer Krylov to rtol 1e-8, preconditioned by the geometric V-cycle with
-    Chebyshev-Jacobi smoothing (or single-level Chebyshev-Jacobi, --pc) in
-    FP64 vs FP32.  Prints one JSON line with both solves and the solutions'
-    difference."""
+def solve_leg(op, m, eta, mask, args, check=True):
+    """Precision form on the op's box: A11 u = f (f uniform [-1, 1] on free
+    dofs), FP64 outer Krylov (args.ksp) to rtol args.rtol, preconditioned by the
+    geometric V-cycle with Chebyshev-Jacobi smoothing (args.pc) in FP64 and in
+    FP32.  Each solver is set up first (levels, eigenvalue estimates, the
+    V-cycle graph: one PCApply, timed apart), then one solve is timed.  With
+    check=True the true residual of each solution comes from the reference's
+    own A11 on the host, and the FP32-smoothed solution's error is stated
+    against the FP64-smoothed one."""
     import torch
 
-    from pt_b200 import MatStokesMF
     from pt_b200 import mesh as M
     from pt_b200.solver import KSPSolveA11
-    torch.cuda.set_device(0)
-    m, eta, mask = M.problem(args.workload, seed=0)
     f = M.uniform_vec(m.nvel, 11)
     f[mask.astype(bool)] = 0.0
-    fd = torch.from_numpy(f).cuda()
-    op = MatStokesMF(*m.dims)
-    op.SetUp(m.coords, eta, mask)
-    # the fine level's tile schedule from the autotuner, as in the apply bench
-    lz, _ = op.autotune_tiling(fd) if not args.no_autotune else (op.tiling, None)
-    out = {"mode": "solve", "workload": args.workload, "nvel": m.nvel, "ksp": args.ksp, "pc": args.pc,
-           "cheby_degree": args.cheby_degree, "rtol": args.rtol, "tiling_lz": lz}
+    fd = torch.from_numpy(f).to(torch.device("cuda", torch.cuda.current_device()))
+    out = {"workload": f"{m.mx}x{m.my}x{m.mz} box of the apply leg", "nvel": m.nvel, "ksp": args.ksp,
+           "pc": args.pc, "cheby_degree": args.cheby_degree, "rtol": args.rtol, "tiling_lz": op.tiling}
     sols = {}
     for name, fp32 in (("fp64", 0), ("fp32_smoothed", 1)):
         x = torch.zeros_like(fd)
         with KSPSolveA11(op, ksp=args.ksp, pc=args.pc, cheby_degree=args.cheby_degree, cheby_fp32=fp32,
                          rtol=args.rtol, max_it=args.max_it, restart=args.restart) as k:
-            first = k.solve(fd, x)   # builds levels, estimates eigenvalues, warms up
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            k.apply_pc(fd, x)   # PCSetUp + one V-cycle
+            torch.cuda.synchronize()
+            t_setup = time.perf_counter() - t0
             x.zero_()
             st = k.solve(fd, x)
-            st["first_solve_seconds_incl_setup"] = first["seconds"]
-        sols[name] = x
+        st["setup_seconds"] = t_setup
+        sols[name] = x.cpu().numpy()
+        del x
         out[name] = st
-    d = (sols["fp32_smoothed"] - sols["fp64"]).abs().max().item() / sols["fp64"].abs().max().item()
-    out["solution_relerr_fp32_vs_fp64"] = d
+    out["solution_relerr_fp32_vs_fp64"] = _relerr(sols["fp32_smoothed"], sols["fp64"])
     out["time_to_solution_speedup"] = out["fp64"]["seconds"] / out["fp32_smoothed"]["seconds"]
+    if check:
+        for name in sols:
+            out[name]["true_relres_reference_a11"] = reference_residual(m, eta, mask, f, sols[name])
+    return out
+
+
+def run_solve(args):
+    """--mode solve: the precision-form leg alone on args.workload; prints one
+    JSON line."""
+    import torch
+
+    from pt_b200 import MatStokesMF
+    from pt_b200 import mesh as M
+    torch.cuda.set_device(0)
+    m, eta, mask = M.problem(args.workload, seed=0)
+    op = MatStokesMF(*m.dims)
+    op.SetUp(m.coords, eta, mask)
+    if not args.no_autotune:
+        op.autotune_tiling(torch.from_numpy(M.uniform_vec(m.nvel, 7)).cuda())
+    out = {"mode": "solve", "workload": args.workload}
+    out.update(solve_leg(op, m, eta, mask, args, check=not args.no_cpu_baseline))
     print(json.dumps(out))
     op.Destroy()
     return 0
@@ -460,15 +538,14 @@ def batched_problems(n=256, seed=0):
     return out
 
 
-def run_batched(args):
+def batched_leg(nbatch, steps):
     """Batched form: one batched A11 apply over all problems (work-list
     launches) vs the same problems applied one after another, FP64 and FP32."""
     import torch
 
     from pt_b200 import MatStokesMF
     from pt_b200.batch import BatchA11, autotune_lz
-    torch.cuda.set_device(0)
-    probs = batched_problems(args.nbatch, seed=0)
+    probs = batched_problems(nbatch, seed=0)
     ops, us64 = [], []
     for i, (m, eta, mask) in enumerate(probs):
         op = MatStokesMF(*m.dims)
@@ -495,23 +572,30 @@ def run_batched(args):
         ys = [torch.empty_like(u) for u in us]
         best, table = autotune_lz(ops, us, ys)
         with BatchA11(ops, lz=best if best else None) as b:
-            t_b = timed(lambda: b.apply(us, ys, masked=True), args.steps)
+            t_b = timed(lambda: b.apply(us, ys, masked=True), steps)
             launches = b.launches_per_apply
         # sequential baselines: each box's own default apply ("b200": stored element
         # matrices up to 32^3, else streaming), and the streaming kernel the batch runs
-        t_s = timed(lambda: [op.MatMult_MFStokes_A11(u, y) for op, u, y in zip(ops, us, ys)], max(2, args.steps // 4))
+        t_s = timed(lambda: [op.MatMult_MFStokes_A11(u, y) for op, u, y in zip(ops, us, ys)], max(2, steps // 4))
         for op in ops:
             op.set_a11_op("b200_stream")
-        t_ss = timed(lambda: [op.MatMult_MFStokes_A11(u, y) for op, u, y in zip(ops, us, ys)], max(2, args.steps // 4))
+        t_ss = timed(lambda: [op.MatMult_MFStokes_A11(u, y) for op, u, y in zip(ops, us, ys)], max(2, steps // 4))
         for op in ops:
             op.set_a11_op("b200")
         out[prec] = {"batched_ms": t_b, "sequential_ms": t_s, "batched_gdofs": ndof / t_b / 1e6,
                      "sequential_gdofs": ndof / t_s / 1e6, "speedup": t_s / t_b,
                      "sequential_stream_ms": t_ss, "speedup_vs_sequential_stream": t_ss / t_b,
                      "launches_per_apply": launches, "autotune_lz": best, "autotune_ms": table}
-    print(json.dumps(out))
     for op in ops:
         op.Destroy()
+    return out
+
+
+def run_batched(args):
+    """--mode batched: the batched leg alone; prints one JSON line."""
+    import torch
+    torch.cuda.set_device(0)
+    print(json.dumps(batched_leg(args.nbatch, args.steps)))
     return 0
 
 
@@ -567,19 +651,19 @@ def serve_run(reqs, arrivals, iters, **opts):
     return res, st
 
 
-def run_serve(args):
+def serve_leg(args, nreq, ncal, nserial):
     """Serving form: Poisson arrivals at ~80% of the measured capacity, solves
     of A11 u = f to rtol 1e-8 by FP32 Chebyshev(3)-Jacobi-preconditioned FP64
     CG, continuously batched; p50/p99 latency and solves/s against serial
-    plain FP64 solves of the same requests."""
+    plain FP64 solves of the same requests.  The true FP64 residual of a sample
+    of served results comes from the reference's own A11 on the host."""
     import torch
 
     from pt_b200 import MatStokesMF
     from pt_b200.solver import KSPSolveA11
-    torch.cuda.set_device(0)
     t_gen = time.time()
-    cal = serve_requests(args.ncal, seed=1)
-    reqs = serve_requests(args.nreq, seed=0)
+    cal = serve_requests(ncal, seed=1)
+    reqs = serve_requests(nreq, seed=0)
     t_gen = time.time() - t_gen
     # tile schedule (tile width, z-chunk depth) by the autotuner, on the
     # calibration requests' FP32 applies
@@ -612,13 +696,10 @@ def run_serve(args):
     relres = []
     for i in range(0, len(reqs), max(1, len(reqs) // 8)):
         m, eta, mask, f, _ = reqs[i]
-        with MatStokesMF(*m.dims) as op:
-            op.SetUp(m.coords, eta, mask)
-            y = op.MatMult_MFStokes_A11(torch.from_numpy(res[i]["x"]).cuda()).cpu().numpy()
-        relres.append(float(np.linalg.norm(f - y) / np.linalg.norm(f)))
+        relres.append(reference_residual(m, eta, mask, f, res[i]["x"]))
     # serial plain FP64 solves (one request at a time, set-up included)
     serial = []
-    for i in np.linspace(0, len(reqs) - 1, min(args.nserial, len(reqs))).astype(int):
+    for i in np.linspace(0, len(reqs) - 1, min(nserial, len(reqs))).astype(int):
         m, eta, mask, f, _ = reqs[i]
         torch.cuda.synchronize()
         t = time.time()
@@ -645,7 +726,15 @@ def run_serve(args):
            "speedup_solves_per_s": (len(reqs) / wall) / serial_rate, "server": st,
            "autotune": {"lz": lz, "tile_x": tile_x, "ms": {f"lz{a}_tx{b}": v for (a, b), v in table.items()}},
            "host_generation_s": t_gen}
-    print(json.dumps(out))
+    return out
+
+
+def run_serve(args):
+    """--mode serve: the served stream alone (args.nreq requests); prints one
+    JSON line."""
+    import torch
+    torch.cuda.set_device(0)
+    print(json.dumps(serve_leg(args, args.nreq, args.ncal, args.nserial)))
     return 0
 
 
@@ -718,7 +807,12 @@ def main():
     ap.add_argument("--nserial", type=int, default=12, help="serve: requests solved one at a time")
     ap.add_argument("--serve-iters", type=int, default=8, help="serve: iterations per server step")
     ap.add_argument("--nbatch", type=int, default=256)
-    ap.add_argument("--ksp", default="fgmres")
+    ap.add_argument("--no-legs", action="store_true",
+                    help="apply mode: skip the solve / batched / served legs of the default line")
+    ap.add_argument("--leg-nreq", type=int, default=100, help="served leg of the default line: requests")
+    ap.add_argument("--leg-ncal", type=int, default=32, help="served leg: capacity calibration requests")
+    ap.add_argument("--leg-nserial", type=int, default=8, help="served leg: requests solved one at a time")
+    ap.add_argument("--ksp", default="fcg")
     ap.add_argument("--rtol", type=float, default=1e-8)
     ap.add_argument("--max-it", type=int, default=20000)
     ap.add_argument("--restart", type=int, default=30)

@@ -33,9 +33,25 @@ _u8p = ctypes.POINTER(ctypes.c_uint8)
 _i32p = ctypes.POINTER(ctypes.c_int32)
 
 
+def reference_tree():
+    """The reference source tree to compile Route A from: $PTATIN_REF_DIR, else
+    a ``reference`` directory beside this repository; None when neither has
+    the reference's ``src/``."""
+    cands = [os.environ.get("PTATIN_REF_DIR", ""),
+             os.path.join(os.path.dirname(os.path.dirname(_HERE)), "reference")]
+    for c in cands:
+        if c and os.path.isdir(os.path.join(c, "src")):
+            return c
+    return None
+
+
 def build(quiet: bool = True) -> None:
     """Compile liboracle.so (and _ref/libptref.so where the reference exists)."""
-    out = subprocess.run(["make", "-C", _HERE, "all"], capture_output=True, text=True)
+    cmd = ["make", "-C", _HERE, "all"]
+    ref = reference_tree()
+    if ref:
+        cmd.append(f"REF={ref}")
+    out = subprocess.run(cmd, capture_output=True, text=True)
     if out.returncode != 0:
         raise RuntimeError("oracle build failed:\n" + out.stdout + out.stderr)
     if not quiet:
@@ -269,3 +285,50 @@ class RefCPU:
         self._check(self.lib.ref_a12(self.KINDS[kind], mx, my, mz, _ptr(_f64(coords)),
                                      _ptr(p), _ptr(y)), "A12")
         return y
+
+    # ---- MatShell level: the reference's element loops with the BC rules of
+    # src/stokes_operators.c (one rank, so local = global) -------------------
+    def matmult_a11(self, dims, coords, eta, mask, x, kind="avx"):
+        """MatMult_MFStokes_A11 (stokes_operators.c:1156-1222): Dirichlet entries
+        of the local input zeroed (BCListInsertLocalZero), the back-end's
+        element loop, then y_k = x_k on Dirichlet dofs
+        (BCListInsertDirichlet_MatMult, scale 1)."""
+        m = _mask(mask).astype(bool)
+        xz = _f64(x).copy()
+        xz[m] = 0.0
+        y = self.a11(dims, coords, eta, xz, kind)
+        y[m] = _f64(x)[m]
+        return y
+
+    def getdiag_a11(self, dims, coords, eta, mask):
+        """MatGetDiagonal_MFStokes_A11 (stokes_operators.c:1072-1113): the
+        element diagonal, 1.0 in Dirichlet slots
+        (BCListInsertValueIntoDirichletSlot)."""
+        d = self.diag(dims, coords, eta)
+        d[_mask(mask).astype(bool)] = 1.0
+        return d
+
+    def matmult_a12(self, dims, coords, mask, p, kind="avx"):
+        """MatMult_MFStokes_A12 (stokes_operators.c:1301-1370): B^T p with the
+        velocity Dirichlet rows zeroed (BCListInsertZero)."""
+        y = self.a12(dims, coords, p, kind)
+        y[_mask(mask).astype(bool)] = 0.0
+        return y
+
+    def matmult_a21(self, dims, coords, mask, u):
+        """MatMult_MFStokes_A21 (stokes_operators.c:1444-1509): B u with the
+        Dirichlet entries of u zeroed; no pressure BC."""
+        uz = _f64(u).copy()
+        uz[_mask(mask).astype(bool)] = 0.0
+        return self.a21(dims, coords, uz)
+
+    def matmult_a(self, dims, coords, eta, mask, u, p, kind="avx"):
+        """MatMult_MFStokes_A (stokes_operators.c:893-979): Dirichlet columns of
+        u zeroed, Yu = A11 u + A12 p and Yp = A21 u in one element loop
+        (MFStokesWrapper_A[_AVX]), then Yu_k = u_k on Dirichlet dofs."""
+        m = _mask(mask).astype(bool)
+        uz = _f64(u).copy()
+        uz[m] = 0.0
+        yu, yp = self.stokes_a(dims, coords, eta, uz, p, kind)
+        yu[m] = _f64(u)[m]
+        return yu, yp

@@ -35,16 +35,8 @@ template <typename T, int TX, bool MASKED>
 pt_status batch_launch_cls(const pt_batch *b, const pt_batch::Cls &c, const T *const *u, T *const *y, cudaStream_t st)
 {
   constexpr size_t smem = ptk::stream_smem_bytes<T, TX>();
-  static bool attr_set[64] = {false};
-  int dev = 0;
-  PT_CUDA(cudaGetDevice(&dev));
-  if (dev < 64 && !attr_set[dev]) {
-    PT_CUDA(cudaFuncSetAttribute(ptk::a11_stream_batch_kernel<T, TX, MASKED>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    PT_CUDA(cudaFuncSetAttribute(ptk::a11_stream_batch_kernel<T, TX, MASKED>,
-                                 cudaFuncAttributePreferredSharedMemoryCarveout, (int)cudaSharedmemCarveoutMaxShared));
-    attr_set[dev] = true;
-  }
+  pt_status as = kernel_attrs((const void *)ptk::a11_stream_batch_kernel<T, TX, MASKED>, smem);
+  if (as != PT_OK) return as;
   const ptk::BatchProb *probs = std::is_same<T, double>::value ? b->d_probs64 : b->d_probs32;
   ptk::a11_stream_batch_kernel<T, TX, MASKED>
       <<<(unsigned)c.count, TX, smem, st>>>(probs, b->d_items + c.off, c.px, c.py, c.pz, u, y);

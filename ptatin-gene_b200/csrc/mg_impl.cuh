@@ -141,8 +141,10 @@ __global__ void eta_from_vertex_kernel(MgBox b, const double *__restrict__ vf, d
 pt_status upload_q1_table()
 {
   static bool done[64] = {false};
+  static std::mutex mu;
   int dev = 0;
   PT_CUDA(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lock(mu);
   if (dev < 64 && done[dev]) return PT_OK;
   const double g[3] = {-q2::GS, 0.0, q2::GS};
   double t[27][8];

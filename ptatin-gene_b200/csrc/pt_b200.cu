@@ -157,6 +157,28 @@ unsigned grid_stride_blocks(int64_t n)
   return (unsigned)(b < 148 * 16 ? (b < 1 ? 1 : b) : 148 * 16);
 }
 
+// One-time, per-device set-up of a kernel's launch attributes: the dynamic
+// shared-memory limit (smem > 0) and, for the tiled kernels, the largest shared-memory
+// carve-out (so every entry point launches a kernel at the same occupancy).
+// Guarded by a mutex: host threads may launch on several devices at once.
+std::mutex g_attr_mu;
+std::vector<std::pair<const void *, int>> g_attr_done;
+
+pt_status kernel_attrs(const void *fn, size_t smem, bool max_carveout = true)
+{
+  int dev = 0;
+  PT_CUDA(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lock(g_attr_mu);
+  for (const auto &d : g_attr_done)
+    if (d.first == fn && d.second == dev) return PT_OK;
+  if (smem) PT_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  if (max_carveout)
+    PT_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                 (int)cudaSharedmemCarveoutMaxShared));
+  g_attr_done.push_back({fn, dev});
+  return PT_OK;
+}
+
 pt_status check_ready(const pt_op *op, bool need_eta)
 {
   if (!op) return fail(PT_ERR_BAD_ARG, "op is NULL");
@@ -168,8 +190,10 @@ pt_status check_ready(const pt_op *op, bool need_eta)
 pt_status upload_diag_tables()
 {
   static bool done[64] = {false};
+  static std::mutex mu;
   int dev = 0;
   PT_CUDA(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lock(mu);
   if (dev < 64 && done[dev]) return PT_OK;
   // dN_n/dxi_d at Gauss point q (tensor-product Q2 basis).
   double b[3][3], db[3][3];
@@ -209,14 +233,8 @@ pt_status launch_stream_tx(pt_op *op, const T *K, const T *u, T *y, int zb = 0, 
 {
   if (ze < 0) ze = op->nzc;
   constexpr size_t smem = ptk::stream_smem_bytes<T, TX>();
-  static bool attr_set[64] = {false};
-  if (op->device < 64 && !attr_set[op->device]) {
-    PT_CUDA(cudaFuncSetAttribute(ptk::a11_stream_kernel<T, TX, MASKED>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)smem));
-    PT_CUDA(cudaFuncSetAttribute(ptk::a11_stream_kernel<T, TX, MASKED>,
-                                 cudaFuncAttributePreferredSharedMemoryCarveout, (int)cudaSharedmemCarveoutMaxShared));
-    attr_set[op->device] = true;
-  }
+  pt_status as = kernel_attrs((const void *)ptk::a11_stream_kernel<T, TX, MASKED>, smem);
+  if (as != PT_OK) return as;
   ptk::StreamGrid g;
   g.b = op->box;
   g.TX = TX; g.ntx = op->ntx; g.LZ = op->LZ; g.nzc = op->nzc; g.MXP = op->MXP;
@@ -240,11 +258,8 @@ template <bool MASKED>
 pt_status launch_tmem(pt_op *op, const double *K, const double *u, double *y)
 {
   constexpr size_t smem = ptk::tmem_smem_bytes();
-  static bool attr_set[64] = {false};
-  if (op->device < 64 && !attr_set[op->device]) {
-    PT_CUDA(cudaFuncSetAttribute(ptk::a11_tmem_kernel<MASKED>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    attr_set[op->device] = true;
-  }
+  pt_status as = kernel_attrs((const void *)ptk::a11_tmem_kernel<MASKED>, smem, false);
+  if (as != PT_OK) return as;
   ptk::StreamGrid g;
   g.b = op->box;
   g.TX = 128; g.ntx = op->ntx; g.LZ = op->LZ; g.nzc = op->nzc; g.MXP = op->MXP;
@@ -341,14 +356,9 @@ const float *op_Ae<float>(const pt_op *op) { return op->d_Ae32; }
 // The element GEMV stages 13-27 KB per CTA: ask for the largest shared-memory
 // carve-out so that 8 (FP64) to 16 (FP32) elements run per SM.
 template <typename T, bool MASKED>
-void ebe_carveout()
+pt_status ebe_carveout()
 {
-  static bool done[64] = {false};
-  int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev >= 64 || done[dev]) return;
-  cudaFuncSetAttribute(ptk::ebe_apply_kernel<T, MASKED>, cudaFuncAttributePreferredSharedMemoryCarveout,
-                       (int)cudaSharedmemCarveoutMaxShared);
-  done[dev] = true;
+  return kernel_attrs((const void *)ptk::ebe_apply_kernel<T, MASKED>, 0, true);
 }
 
 template <typename T>
@@ -356,8 +366,7 @@ pt_status launch_ebe(pt_op *op, const T *u, T *y, bool masked)
 {
   pt_status s = ensure_ebe(op);
   if (s != PT_OK) return s;
-  ebe_carveout<T, true>();
-  ebe_carveout<T, false>();
+  if ((s = ebe_carveout<T, true>()) != PT_OK || (s = ebe_carveout<T, false>()) != PT_OK) return s;
   T *ye = reinterpret_cast<T *>(op->d_ye);
   if (masked) {
     ptk::ebe_apply_kernel<T, true><<<(unsigned)op->nel, 96, 0, op->stream>>>(op->box, op_Ae<T>(op), u, op->d_mask, ye);
@@ -1278,8 +1287,8 @@ pt_status noalloc_launch(const ptk::StreamGrid &g0, int my, const double *K, con
                          cudaStream_t stream)
 {
   constexpr size_t smem = ptk::stream_smem_bytes<double, TX>();
-  PT_CUDA(cudaFuncSetAttribute(ptk::a11_stream_kernel<double, TX, false>,
-                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  pt_status as = kernel_attrs((const void *)ptk::a11_stream_kernel<double, TX, false>, smem);
+  if (as != PT_OK) return as;
   ptk::StreamGrid g = g0;
   for (int pz = 0; pz < 2; pz++)
     for (int py = 0; py < 2; py++)

@@ -561,15 +561,10 @@ constexpr int64_t MG_GALERKIN_MAX_ELEMENTS = 262144;  // Galerkin levels up to 6
 // matrices below that (OP_TYPE_GALERKIN).  Levels above stay re-discretised.
 pt_status mg_galerkin(pt_mg &mg)
 {
-  static bool attr_set[64] = {false};
-  int dev = 0;
-  PT_CUDA(cudaGetDevice(&dev));
   constexpr size_t smem = ptk::galerkin_smem_bytes();
-  if (dev < 64 && !attr_set[dev]) {
-    PT_CUDA(cudaFuncSetAttribute(ptk::galerkin_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    PT_CUDA(cudaFuncSetAttribute(ptk::galerkin_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    attr_set[dev] = true;
-  }
+  pt_status as = kernel_attrs((const void *)ptk::galerkin_kernel<true>, smem, false);
+  if (as == PT_OK) as = kernel_attrs((const void *)ptk::galerkin_kernel<false>, smem, false);
+  if (as != PT_OK) return as;
   for (size_t l = 1; l < mg.lv.size(); l++) {
     pt_mg_level &F = mg.lv[l - 1], &C = mg.lv[l];
     if (!F.Ae64 && C.op->nel > MG_GALERKIN_MAX_ELEMENTS) continue;

@@ -53,3 +53,22 @@ def test_batched_equals_individual(problems, lz, masked, fp32):
         else:
             tol = 1e-5 if fp32 else 1e-14
             assert float((y - ref).abs().max()) <= tol * float(ref.abs().max())
+
+
+def test_batched_matches_oracle(problems, ora):
+    """The batched work-list against the oracle directly (MatShell level, FP64),
+    not only against each box's own apply."""
+    import torch
+
+    from conftest import relerr
+    from pt_b200.batch import BatchA11
+    ops, us = problems
+    ys = [torch.full_like(u, float("nan")) for u in us]
+    with BatchA11(ops) as b:
+        b.apply(us, ys, masked=True)
+        torch.cuda.synchronize()
+    for i, ((mx, my, mz), u, y) in enumerate(zip(SHAPES, us, ys)):
+        m = M.make_mesh(mx, my, mz, perturb=0.05, seed=i)
+        eta = M.eta_per_element(m, contrast=10.0 ** (2 + 2 * (i % 3)), seed=i)
+        ref = ora.matmult_a11(m.dims, m.coords, eta, M.bc_mask_freeslip(mx, my, mz), u.cpu().numpy())
+        assert relerr(y.cpu().numpy(), ref) < 1e-12, (mx, my, mz)

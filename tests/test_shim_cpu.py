@@ -9,8 +9,10 @@ from conftest import REPO
 
 
 def test_shim_compiles_against_reference_headers():
-    out = subprocess.run(["make", "-s", "-C", os.path.join(REPO, "oracle"), "shim-check"],
-                         capture_output=True, text=True)
+    import oracle
+    ref = oracle.reference_tree()
+    cmd = ["make", "-s", "-C", os.path.join(REPO, "oracle"), "shim-check"] + ([f"REF={ref}"] if ref else [])
+    out = subprocess.run(cmd, capture_output=True, text=True)
     if "skipped" in out.stdout:
         pytest.skip(out.stdout.strip())
     assert out.returncode == 0, out.stdout + out.stderr

@@ -3,8 +3,9 @@ device memory when they need it (a process that gave the GPU to its own
 fixed-size pool, or runs under an exhausted memory cap, or must not stall on
 the allocator).  It keeps its geometry scratch in a fixed device array, so it
 is checked here against the op-based entry point that allocates (pt_a11_apply_d)
-on two calls in a row -- the scratch keeps the previous call's contents, which
-must not leak into the next result.  This file is collected last on purpose."""
+and against the oracle's A11 (the reference's tensor-path arithmetic) on two
+calls in a row -- the scratch keeps the previous call's contents, which must
+not leak into the next result.  This file is collected last on purpose."""
 import ctypes
 
 import numpy as np
@@ -22,7 +23,7 @@ def _desc(dims):
 
 
 @pytest.mark.gpu
-def test_noalloc_apply_matches_op_apply_twice():
+def test_noalloc_apply_matches_op_apply_twice(ora):
     import torch
 
     from pt_b200 import MatStokesMF, _capi
@@ -32,7 +33,8 @@ def test_noalloc_apply_matches_op_apply_twice():
     # two different meshes and inputs in a row through the same scratch
     for workload, seed in (("box:16,16,16", 3), ("box:9,5,7", 4)):
         m, eta, _ = M.problem(workload, seed=seed)
-        u = torch.from_numpy(M.uniform_vec(m.nvel, seed + 10)).cuda()
+        uh = M.uniform_vec(m.nvel, seed + 10)
+        u = torch.from_numpy(uh).cuda()
         c = torch.from_numpy(m.coords).cuda()
         e = torch.from_numpy(eta).cuda()
         y = torch.full((m.nvel,), float("nan"), dtype=torch.float64, device="cuda")
@@ -45,6 +47,7 @@ def test_noalloc_apply_matches_op_apply_twice():
             ref = op.MFStokesWrapper_A11(u)
         torch.cuda.synchronize()
         assert relerr(y.cpu().numpy(), ref.cpu().numpy()) < TOL64
+        assert relerr(y.cpu().numpy(), ora.a11(m.dims, m.coords, eta, uh)) < TOL64
 
 
 def test_noalloc_rejects_meshes_beyond_its_scratch():
