@@ -252,6 +252,8 @@ pt_status pt_batch_create(int n, pt_op *const *ops, const int32_t *lz, pt_batch 
  * batch in one class per colour, fewer launches per apply. */
 pt_status pt_batch_create_tiled(int n, pt_op *const *ops, const int32_t *lz, int32_t tile_x, pt_batch **batch);
 pt_status pt_batch_destroy(pt_batch *batch);
+/* Colour-class launches of one apply (a masked apply adds one launch for the
+ * Dirichlet rows of every problem). */
 int64_t pt_batch_launches_per_apply(const pt_batch *batch);
 int64_t pt_batch_tiles(const pt_batch *batch);
 /* y_i = A11_i u_i for every problem; u, y are DEVICE arrays of n device
@@ -344,6 +346,27 @@ pt_status pt_project_markers_d(pt_op *op, int64_t n, const int32_t *wil, const d
 pt_status pt_project_markers_h(pt_op *op, int64_t n, const int32_t *wil, const double *xi, const double *eta,
                                const double *rho, double *eta_qp, double *rho_qp, int install);
 
+/* ---- momentum residual ------------------------------------------------------ */
+
+/* Gauss-point body force QPntVolCoefStokes.Fu (include/QPntVolCoefStokes_def.h:
+ * 41-46), [27 nel][3] in the viscosity's element-major, point-minor order.
+ * The strided form reads three consecutive doubles per record, records
+ * `stride` doubles apart: &qp[0].Fu[0] with stride 6 for the reference's
+ * 48-byte records. */
+pt_status pt_op_set_body_force_h(pt_op *op, const double *fu);
+pt_status pt_op_set_body_force_d(pt_op *op, const double *fu);
+pt_status pt_op_set_body_force_strided_h(pt_op *op, const double *fu0, int64_t stride);
+/* Replaces FormFunctionLocal_U (src/stokes_form_function.c:99-243): the
+ * unassembled local momentum residual ru = A11 u + A12 p - F, where F[n,l] =
+ * sum_q w detJ N_n(q) Fu_l(q) is the body-force load.  u is the ghosted local
+ * velocity as given (the caller has inserted the Dirichlet values,
+ * BCListInsertLocal; no column is zeroed), p the element-local pressure; the
+ * caller does the local-to-global ADD and BCListResidualDirichlet, as
+ * FormFunction_Stokes (:478-580) does.  ru is overwritten.  The load vector F
+ * is formed on first use after the coordinates or the body force change. */
+pt_status pt_residual_u_d(pt_op *op, const double *u, const double *p, double *ru);
+pt_status pt_residual_u_h(pt_op *op, const double *u, const double *p, double *ru);
+
 /* ---- selection, in the style of -a11_op --------------------------------- */
 
 /* Select the A11 kernel by name, like the reference's -a11_op function list
@@ -351,9 +374,7 @@ pt_status pt_project_markers_h(pt_op *op, int64_t n, const int32_t *wil, const d
  * matrices for one-rank boxes of at most 32768 elements, the streaming kernel
  * above), "b200_stream" (the streaming kernel with precomputed Gauss-point
  * geometry), "b200_ebe" (stored 81x81 element matrices, element GEMV + node
- * gather; one-rank boxes), "b200_tmem" (the streaming kernel with TMEM
- * accumulators, FP64 rows of 65..128 elements) and "b200_colour" (8-colour
- * element kernel).  The getter returns the kernel in use.  Unknown names give
+ * gather; one-rank boxes) and "b200_colour" (8-colour element kernel).  The getter returns the kernel in use.  Unknown names give
  * PT_ERR_BAD_ARG, as the reference's SETERRQ1 "No -a11_op %s". */
 pt_status pt_op_set_a11_kernel(pt_op *op, const char *name);
 const char *pt_op_get_a11_kernel(const pt_op *op);

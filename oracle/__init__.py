@@ -91,6 +91,7 @@ class Oracle:
         L.ora_matmult_a12.argtypes = [i, i, i, _dp, _u8p, _dp, _dp, i]
         L.ora_matmult_a21.argtypes = [i, i, i, _dp, _u8p, _dp, _dp]
         L.ora_a11_flops.argtypes = [ctypes.c_int64]
+        L.ora_residual_u.argtypes = [i, i, i, _dp, _dp, _dp, _dp, _dp, _dp]
         L.ora_marker_project.argtypes = [i, i, i, ctypes.c_int64, _i32p, _dp, _dp, _dp, _dp, _dp]
         L.ora_a11_flops.restype = ctypes.c_double
         L.ora_num_threads.restype = ctypes.c_int
@@ -171,6 +172,15 @@ class Oracle:
         yu[m] = _f64(u)[m]
         return yu, yp
 
+    def residual_u(self, dims, coords, eta, fu, u, p):
+        """FormFunctionLocal_U (src/stokes_form_function.c:99-243): unassembled
+        local Ru = A11 u + A12 p - body force; fu is [27 nel][3]."""
+        mx, my, mz = dims
+        ru = np.zeros_like(_f64(u))
+        self.lib.ora_residual_u(mx, my, mz, _ptr(_f64(coords)), _ptr(_f64(eta)), _ptr(_f64(fu)), _ptr(_f64(u)),
+                                _ptr(_f64(p)), _ptr(ru))
+        return ru
+
     def marker_project(self, dims, wil, xi, eta, rho):
         """Gauss-point (eta, rho) from markers (restatement of the reference's
         Q1 projection, src/material_point_utils.c:957-1190)."""
@@ -218,6 +228,7 @@ class RefCPU:
         L.ref_a12.argtypes = [i, i, i, i, _dp, _dp, _dp]
         L.ref_stokes_a.argtypes = [i, i, i, i, _dp, _dp, _dp, _dp, _dp, _dp]
         L.ref_marker_project.argtypes = [i, i, i, i, ctypes.POINTER(ctypes.c_int), _dp, _dp, _dp, _dp, _dp]
+        L.ref_residual_u.argtypes = [i, i, i, _dp, _dp, _dp, _dp, _dp, _dp]
         L.ref_has_avx.restype = i
         L.ref_set_threads.argtypes = [i]
         L.ref_set_threads.restype = i
@@ -270,6 +281,18 @@ class RefCPU:
                                                 _ptr(_f64(xi)), _ptr(_f64(eta)), _ptr(_f64(rho)), _ptr(eq),
                                                 _ptr(rq)), "marker projection")
         return eq, rq
+
+    def residual_u(self, dims, coords, eta, fu, u, p):
+        """The reference's own FormFunctionLocal_U (src/stokes_form_function.c:
+        99-243) compiled unmodified: unassembled local Ru = A11 u + A12 p -
+        body force, with fu the Gauss-point QPntVolCoefStokes.Fu ([27 nel][3])."""
+        mx, my, mz = dims
+        u = _f64(u).copy()
+        p = _f64(p).copy()
+        ru = np.zeros_like(u)
+        self._check(self.lib.ref_residual_u(mx, my, mz, _ptr(_f64(coords)), _ptr(_f64(eta)), _ptr(_f64(fu)),
+                                            _ptr(u), _ptr(p), _ptr(ru)), "FormFunctionLocal_U")
+        return ru
 
     def a21(self, dims, coords, u):
         mx, my, mz = dims

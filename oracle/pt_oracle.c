@@ -444,6 +444,79 @@ void ora_a11_ref(int mx, int my, int mz, const double *coords, const double *eta
   }
 }
 
+/*
+ * Momentum residual FormFunctionLocal_U (stokes_form_function.c:99-243) on one
+ * rank, restated: per element and Gauss point, with the ref-path geometry,
+ *   fac = w detJ,  p_q = fac * sum_i Np_i p_i  (P1GRel basis, :163-166),
+ *   strain exx.. from dN/dx (:169-178), stresses 2 eta fac exx, eta fac exy
+ *   (:183-192),
+ *   Fe[3k+0] += dNdx (sxx - p_q) + dNdy sxy + dNdz sxz    (and y, z; :194-198)
+ *   Be[3k+c] += fac N_k Fu_c                               (:201-205)
+ * and Ru += Fe - Be (:209-213).  u is used as given (the caller inserts the
+ * Dirichlet values); fu is the Gauss-point body force, 3 per point.
+ */
+void ora_residual_u(int mx, int my, int mz, const double *coords, const double *eta, const double *fu,
+                    const double *u, const double *pr, double *ru)
+{
+  const int64_t nel = (int64_t)mx * my * mz;
+  double WEIGHT[NQP], XI[NQP][3], GNI[NQP][3][NPE], NI[NQP][NPE];
+  int64_t e;
+  int p;
+  ref_tables(WEIGHT, XI, GNI);
+  for (p = 0; p < NQP; p++) q2_ni(XI[p], NI[p]);
+  for (e = 0; e < nel; e++) {
+    double elc[3 * NPE], ux[NPE], uy[NPE], uz[NPE], Fe[3 * NPE], Be[3 * NPE], NIp[NQP][4];
+    double detJ[NQP], dNdx[NQP][NPE], dNdy[NQP][NPE], dNdz[NQP][NPE];
+    int64_t nid[NPE];
+    int k;
+    element_nodes(mx, my, e, nid);
+    gather_coords(coords, nid, elc);
+    for (k = 0; k < NPE; k++) {
+      ux[k] = u[3 * nid[k]];
+      uy[k] = u[3 * nid[k] + 1];
+      uz[k] = u[3 * nid[k] + 2];
+    }
+    for (p = 0; p < NQP; p++) p1grel_ni(XI[p], elc, NIp[p]);
+    ref_geometry(elc, GNI, detJ, dNdx, dNdy, dNdz);
+    memset(Fe, 0, sizeof Fe);
+    memset(Be, 0, sizeof Be);
+    for (p = 0; p < NQP; p++) {
+      const double fac = WEIGHT[p] * detJ[p], eg = eta[NQP * e + p];
+      double pq = 0.0, exx = 0, eyy = 0, ezz = 0, exy = 0, exz = 0, eyz = 0;
+      double d1, d2, sxx, syy, szz, sxy, sxz, syz;
+      for (k = 0; k < 4; k++) pq += NIp[p][k] * pr[4 * e + k];
+      pq = pq * fac;
+      for (k = 0; k < NPE; k++) {
+        exx += dNdx[p][k] * ux[k];
+        eyy += dNdy[p][k] * uy[k];
+        ezz += dNdz[p][k] * uz[k];
+        exy += dNdy[p][k] * ux[k] + dNdx[p][k] * uy[k];
+        exz += dNdz[p][k] * ux[k] + dNdx[p][k] * uz[k];
+        eyz += dNdz[p][k] * uy[k] + dNdy[p][k] * uz[k];
+      }
+      d1 = 2.0 * eg * fac;
+      d2 = eg * fac;
+      sxx = d1 * exx; syy = d1 * eyy; szz = d1 * ezz;
+      sxy = d2 * exy; sxz = d2 * exz; syz = d2 * eyz;
+      for (k = 0; k < NPE; k++) {
+        Fe[3 * k] += dNdx[p][k] * (sxx - pq) + dNdy[p][k] * sxy + dNdz[p][k] * sxz;
+        Fe[3 * k + 1] += dNdy[p][k] * (syy - pq) + dNdx[p][k] * sxy + dNdz[p][k] * syz;
+        Fe[3 * k + 2] += dNdz[p][k] * (szz - pq) + dNdx[p][k] * sxz + dNdy[p][k] * syz;
+      }
+      for (k = 0; k < NPE; k++) {
+        Be[3 * k] += fac * NI[p][k] * fu[3 * (NQP * e + p)];
+        Be[3 * k + 1] += fac * NI[p][k] * fu[3 * (NQP * e + p) + 1];
+        Be[3 * k + 2] += fac * NI[p][k] * fu[3 * (NQP * e + p) + 2];
+      }
+    }
+    for (k = 0; k < NPE; k++) {
+      ru[3 * nid[k]] += Fe[3 * k] - Be[3 * k];
+      ru[3 * nid[k] + 1] += Fe[3 * k + 1] - Be[3 * k + 1];
+      ru[3 * nid[k] + 2] += Fe[3 * k + 2] - Be[3 * k + 2];
+    }
+  }
+}
+
 /* diag(A11) (stokes_operators_mf.c:71-135, diag_def.c:120-205). */
 void ora_a11_diag(int mx, int my, int mz, const double *coords, const double *eta, double *y)
 {

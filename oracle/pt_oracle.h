@@ -78,6 +78,11 @@ void ora_marker_project(int mx, int my, int mz, int64_t npoints, const int32_t *
                         const double *eta_p, const double *rho_p, double *eta_qp, double *rho_qp);
 double ora_a11_flops(int64_t nel);
 
+/* Momentum residual FormFunctionLocal_U (src/stokes_form_function.c:99-243):
+ * ru += A11 u + A12 p - sum_q w detJ N fu_q; fu holds 3 values per Gauss point. */
+void ora_residual_u(int mx, int my, int mz, const double *coords, const double *eta, const double *fu,
+                    const double *u, const double *pr, double *ru);
+
 /* Number of OpenMP threads the element loops use (1 when built without OpenMP). */
 int ora_num_threads(void);
 

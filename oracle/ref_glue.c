@@ -19,6 +19,8 @@
  *     array of QPntVolCoefStokes built from a plain eta[27*nel].
  *   - PetscDTGaussQuadrature for n=3 (PETSc 3.8.3, absent here): closed form
  *     of the Golub-Welsch result, nodes 0, +-sqrt(3/5), weights 8/9, 5/9.
+ *   - a PhysCompStokes carrying the quadrature for the momentum residual
+ *     FormFunctionLocal_U (src/stokes_form_function.c:99-243);
  *   - for the marker -> Gauss-point viscosity projection of
  *     src/material_point_utils.c: local vectors of a dof-1 Q2 node grid
  *     (DMGetLocalVector ...), local<->global on one rank (identity / add),
@@ -37,6 +39,7 @@
 #include "MPntStd_def.h"
 #include "MPntPStokes_def.h"
 #include "material_point_utils.h"
+#include "private/ptatin3d_stokes_impl.h"
 
 struct _p_Vec {
   PetscScalar *a;
@@ -357,6 +360,33 @@ int ref_stokes_a(int kind, int mx, int my, int mz, const double *coords, const d
 #endif
   if (kind == 2) ierr = MFStokesWrapper_A(&c.volQ, &c.dau, u, &c.dap, p, yu, yp);
   else ierr = 2;
+  ctx_free(&c);
+  return ierr;
+}
+
+/* The momentum residual FormFunctionLocal_U (src/stokes_form_function.c:99-243)
+ * on one rank: Ru += A11 u + A12 p - (body force), element by element with
+ * the reference's own geometry and P1GRel pressure basis; fu[3*q] holds the
+ * Gauss-point body force QPntVolCoefStokes.Fu.  u is used as given (the
+ * caller inserts the Dirichlet values, BCListInsertLocal). */
+PetscErrorCode FormFunctionLocal_U(PhysCompStokes, DM, PetscScalar[], DM, PetscScalar[], PetscScalar[]);
+
+int ref_residual_u(int mx, int my, int mz, const double *coords, const double *eta, const double *fu, double *u,
+                   double *p, double *ru)
+{
+  RefCtx c;
+  struct _p_PhysCompStokes stokes;
+  PetscInt q;
+  int ierr;
+  if (ctx_init(&c, mx, my, mz, coords, eta)) return 1;
+  for (q = 0; q < 27 * (PetscInt)mx * my * mz; q++) {
+    c.qp[q].Fu[0] = fu[3 * q];
+    c.qp[q].Fu[1] = fu[3 * q + 1];
+    c.qp[q].Fu[2] = fu[3 * q + 2];
+  }
+  memset(&stokes, 0, sizeof stokes);
+  stokes.volQ = &c.volQ;
+  ierr = FormFunctionLocal_U(&stokes, &c.dau, u, &c.dap, p, ru);
   ctx_free(&c);
   return ierr;
 }

@@ -76,6 +76,15 @@ typedef struct _p_PetscQuadrature *PetscQuadrature;
 typedef struct _p_PetscSection *PetscSection;
 typedef struct _p_MatNullSpace *MatNullSpace;
 typedef struct _p_PetscSF *PetscSF;
+typedef struct _p_MatMFFD *MatMFFD;
+typedef const char *MatMFFDType;
+#define MATMFFD_WP "wp"
+typedef struct {
+  PetscInt dim, dof, sw;
+  PetscInt mx, my, mz;
+  PetscInt xs, ys, zs, xm, ym, zm;
+  PetscInt gxs, gys, gzs, gxm, gym, gzm;
+} DMDALocalInfo;
 
 #define PETSC_EXTERN extern
 #define PETSC_STATIC_INLINE static inline
@@ -129,12 +138,14 @@ PetscErrorCode VecGetArray(Vec, PetscScalar **);
 PetscErrorCode VecRestoreArray(Vec, PetscScalar **);
 PetscErrorCode PetscTime(PetscLogDouble *);
 
-/* Declarations only, for compile checks of code written against PETSc (the
- * b200 plug-in shim); nothing here implements them. */
+/* Declarations for code written against PETSc (the b200 plug-in shim); the
+ * shim's test build implements them in shim_host.c, the Route-A build does
+ * not use them. */
 PetscErrorCode DMDAGetGhostCorners(DM, PetscInt *, PetscInt *, PetscInt *, PetscInt *, PetscInt *, PetscInt *);
 PetscErrorCode PetscObjectQuery(PetscObject, const char[], PetscObject *);
 PetscErrorCode PetscObjectCompose(PetscObject, const char[], PetscObject);
 PetscErrorCode PetscObjectStateGet(PetscObject, PetscObjectState *);
+PetscErrorCode PetscObjectReference(PetscObject);
 MPI_Comm PetscObjectComm(PetscObject);
 PetscErrorCode PetscContainerCreate(MPI_Comm, PetscContainer *);
 PetscErrorCode PetscContainerSetPointer(PetscContainer, void *);

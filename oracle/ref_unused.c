@@ -54,3 +54,37 @@ int ptatinDataFieldAccessPoint(void) { return 73; }
 int ptatinDataFieldGetAccess(void) { return 73; }
 int ptatinDataFieldRestoreAccess(void) { return 73; }
 int ptatinDataFieldVerifyAccess(void) { return 73; }
+
+/* Referenced by src/stokes_form_function.c outside FormFunctionLocal_U (the
+ * SNES residual / matrix-free Jacobian drivers and their PETSc plumbing). */
+int BCListInsertDirichlet_MatMult(void) { return 73; }
+int BCListInsertLocal(void) { return 73; }
+int BCListInsertLocalZero(void) { return 73; }
+int BCListResidualDirichlet(void) { return 73; }
+int DMCompositeGather(void) { return 73; }
+int DMCompositeGetAccess(void) { return 73; }
+int DMCompositeGetEntries(void) { return 73; }
+int DMCompositeGetLocalVectors(void) { return 73; }
+int DMCompositeRestoreAccess(void) { return 73; }
+int DMCompositeRestoreLocalVectors(void) { return 73; }
+int DMCompositeScatter(void) { return 73; }
+int DMCreateGlobalVector(void) { return 73; }
+int DMCreateLocalVector(void) { return 73; }
+int DMDAGetLocalInfo(void) { return 73; }
+int DMGetCoordinates(void) { return 73; }
+int MatCreateMFFD(void) { return 73; }
+int MatCreateVecs(void) { return 73; }
+int MatMFFDResetHHistory(void) { return 73; }
+int MatMFFDSetFunction(void) { return 73; }
+int MatMFFDSetType(void) { return 73; }
+int PetscObjectGetComm(void) { return 73; }
+int SurfaceConstraintOps_EvaluateFp(void) { return 73; }
+int SurfaceConstraintOps_EvaluateFu(void) { return 73; }
+int VecAXPY(void) { return 73; }
+int VecCopy(void) { return 73; }
+int VecDuplicate(void) { return 73; }
+int VecGetLocalSize(void) { return 73; }
+int VecGetSize(void) { return 73; }
+int pTatinGetStokesContext(void) { return 73; }
+int pTatinModel_ApplyBoundaryCondition(void) { return 73; }
+int pTatin_EvaluateRheologyNonlinearities(void) { return 73; }

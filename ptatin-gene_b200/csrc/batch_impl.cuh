@@ -45,6 +45,22 @@ pt_status batch_launch_cls(const pt_batch *b, const pt_batch::Cls &c, const T *c
   return PT_OK;
 }
 
+// Dirichlet rows of every masked problem after the colour passes: y_k = x_k
+// (blockIdx.y = problem).
+template <typename T>
+__global__ void batch_bc_kernel(const ptk::BatchProb *__restrict__ probs, const T *const *__restrict__ uptr,
+                                T *const *__restrict__ yptr)
+{
+  const ptk::BatchProb &p = probs[blockIdx.y];
+  if (!p.mask) return;
+  const T *x = uptr[blockIdx.y];
+  T *y = yptr[blockIdx.y];
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < p.nvel; i += (int64_t)gridDim.x * blockDim.x)
+    if (p.mask[i]) y[i] = x[i];
+}
+
+// MASKED: the MatShell apply of every problem with a mask (columns inside the
+// kernel, rows by one more launch).
 template <typename T, bool MASKED>
 pt_status batch_apply(pt_batch *b, const T *const *u, T *const *y, void *stream)
 {
@@ -56,6 +72,12 @@ pt_status batch_apply(pt_batch *b, const T *const *u, T *const *y, void *stream)
     else if (c.TX == 64) s = batch_launch_cls<T, 64, MASKED>(b, c, u, y, st);
     else s = batch_launch_cls<T, 128, MASKED>(b, c, u, y, st);
     if (s != PT_OK) return s;
+  }
+  if (MASKED) {
+    const ptk::BatchProb *probs = std::is_same<T, double>::value ? b->d_probs64 : b->d_probs32;
+    batch_bc_kernel<T><<<dim3(32, (unsigned)b->n), 256, 0, st>>>(probs, u, y);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return fail(PT_ERR_CUDA, "batched Dirichlet rows: %s", cudaGetErrorString(e));
   }
   return PT_OK;
 }
@@ -94,7 +116,10 @@ static pt_status batch_create_impl(int n, pt_op *const *ops, const int32_t *lz, 
     if (L > op->mz) L = op->mz;
     d.LZ = L;
     d.nzc = (op->mz + L - 1) / L;
+    if (op->has_mask && !op->d_mbits) return fail(PT_ERR_STATE, "batch problem %d: mask without its packed bits", i);
     d.mask = op->has_mask ? op->d_mask : nullptr;
+    d.mbits = op->has_mask ? op->d_mbits : nullptr;
+    d.nvel = op->nvel;
     d.K = op->d_K;
     p64[i] = d;
     d.K = op->d_K32;

@@ -309,4 +309,39 @@ __global__ void __launch_bounds__(128) a12_colour_kernel(ColourGrid g, const dou
   }
 }
 
+// ---------------------------------------------------------------------------
+// Body-force load of the momentum residual (src/stokes_form_function.c:201-213):
+//   F[n,l] += sum_q w_q det(J_q) N_n(q) Fu_l(q),  fu = [27 nel][3]
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(128) body_force_colour_kernel(ColourGrid g, const double *__restrict__ coords,
+                                                                const double *__restrict__ fu, double *__restrict__ F)
+{
+  int ei, ej, ek;
+  if (!colour_element(g, (int64_t)blockIdx.x * blockDim.x + threadIdx.x, ei, ej, ek)) return;
+  const int64_t e = ei + (int64_t)g.b.mx * (ej + (int64_t)g.b.my * ek);
+  int64_t nid[27];
+  element_nodes(g.b, ei, ej, ek, nid);
+  double Jg[3][3][27], Xq[3][27];
+  element_jacobian(coords, nid, Jg, Xq);
+  double wd[27];
+#pragma unroll 1
+  for (int q = 0; q < 27; q++) {
+    double J[3][3], adj[3][3];
+#pragma unroll
+    for (int k = 0; k < 3; k++)
+#pragma unroll
+      for (int l = 0; l < 3; l++) J[k][l] = Jg[k][l][q];
+    wd[q] = q2::weight(q) * q2::adjugate(J, adj);
+  }
+#pragma unroll 1
+  for (int l = 0; l < 3; l++) {
+    double r[27], f[27];
+#pragma unroll
+    for (int q = 0; q < 27; q++) r[q] = wd[q] * fu[3 * (27 * e + q) + l];
+    q2::interp_t(r, f);
+#pragma unroll
+    for (int n = 0; n < 27; n++) F[3 * nid[n] + l] += f[n];
+  }
+}
+
 }  // namespace ptk

@@ -26,11 +26,21 @@
 // between two warps goes to a per-warp side buffer.  Completed node planes
 // are flushed to global y once.
 //
+// Data movement.  A layer's two new node planes of u are fetched with
+// cp.async (no registers) into the u slots the finished layer frees, while
+// that layer's completed y planes are flushed; their rows are prefetched to
+// L2 one layer ahead, and each quadrature plane of K one plane ahead.  The
+// MatShell apply's Dirichlet columns come from a packed bit mask whose words
+// are fetched with the plane and applied in shared memory; its Dirichlet rows
+// are set by a separate pass after the colour launches.
+//
 // Determinism across CTAs.  Tiles are coloured by the parity of their x-tile,
 // row and z-chunk index; colours run as separate launches in a fixed order.
 // A node on a tile boundary is stored by the first colour that touches it and
-// read-modify-written by the later ones, so every node's sum has a fixed
-// order and no atomics are used.
+// added to by the later ones (red.global.add: no read-back).  Each launch
+// touches a node from one CTA only and the launches are ordered, so every
+// node's sum is formed in a fixed order: the result is bitwise the same run
+// after run, and the same as a read-modify-write.
 #pragma once
 
 #include <cstdint>
@@ -126,31 +136,102 @@ struct TileLayout {
   }
 };
 
+// Dirichlet bits of the tile's node planes: per slot and plane row, the
+// 32-bit words of the packed mask (bit k = dof k of the local vector) that
+// cover the row's <= 3*(2TX+1) dofs, which start anywhere in a word.
+template <int TX>
+__host__ __device__ constexpr int mask_row_words() { return (3 * (2 * TX + 1) + 31) / 32 + 1; }
+
 template <typename T, int TX>
 constexpr size_t stream_smem_bytes()
 {
   using L = TileLayout<TX>;
-  return sizeof(T) * (2 * (size_t)L::TILE + L::SIDE);
+  return sizeof(T) * (2 * (size_t)L::TILE + L::SIDE) + sizeof(uint32_t) * 9 * mask_row_words<TX>();
 }
 
-// Load node plane p (absolute z node index P) rows 0..2 into slot s.
+// First node of plane-row r of node plane P in the tile starting at element
+// ex0 of row ej.
+__device__ __forceinline__ int64_t row_node0(const StreamGrid &g, int ex0, int ej, int r, int64_t P)
+{
+  return g.b.off + 2 * (int64_t)ex0 + (2 * (int64_t)ej + r) * g.b.X + P * g.b.XY;
+}
+
+// Fetches node plane P (rows 0..2) of u into slot s with asynchronous 4- or
+// 8-byte copies straight into the component-planar tile (cp.async: no
+// registers, the copies run while the thread flushes y); with mbits, also the
+// words of the packed Dirichlet mask that cover each row.  The caller commits
+// and waits.
 template <typename T, int TX, bool MASKED>
-__device__ __forceinline__ void load_plane(T *ut, const StreamGrid &g, int ex0, int ej, int64_t P, int s,
-                                           const T *__restrict__ u, const uint8_t *__restrict__ mask)
+__device__ __forceinline__ void fetch_plane(T *ut, uint32_t *mw, const StreamGrid &g, int ex0, int ej, int64_t P, int s,
+                                            const T *__restrict__ u, const uint32_t *__restrict__ mbits)
 {
   using L = TileLayout<TX>;
-  const int nvalid = min(L::NXN, 2 * (g.b.mx - ex0) + 1);
-  const int nd = 3 * nvalid;
+  const int nd = 3 * min(L::NXN, 2 * (g.b.mx - ex0) + 1);
 #pragma unroll 1
   for (int r = 0; r < 3; r++) {
-    const int64_t node0 = g.b.off + 2 * (int64_t)ex0 + (2 * (int64_t)ej + r) * g.b.X + P * g.b.XY;
-    const T *src = u + 3 * node0;
+    const int64_t k0 = 3 * row_node0(g, ex0, ej, r, P);
+    const T *src = u + k0;
     for (int d = threadIdx.x; d < nd; d += TX) {
-      T v = src[d];
-      if (MASKED && mask[3 * node0 + d]) v = T(0);
       const int n = d / 3, c = d - 3 * n;
-      ut[L::at(c, s, r, n)] = v;
+      const uint32_t dst = (uint32_t)__cvta_generic_to_shared(&ut[L::at(c, s, r, n)]);
+      if (sizeof(T) == 8) asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(dst), "l"(src + d) : "memory");
+      else asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(dst), "l"(src + d) : "memory");
     }
+    if (MASKED && mbits) {
+      const int64_t w0 = k0 >> 5;
+      const int nw = (int)(((k0 + nd - 1) >> 5) - w0 + 1);
+      if ((int)threadIdx.x < nw) {
+        const uint32_t dst = (uint32_t)__cvta_generic_to_shared(&mw[(s * 3 + r) * mask_row_words<TX>() + threadIdx.x]);
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(dst), "l"(mbits + w0 + threadIdx.x) : "memory");
+      }
+    }
+  }
+}
+
+__device__ __forceinline__ void fetch_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void fetch_wait() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+
+// Zeroes the Dirichlet entries of NP node planes P0, P0+1, .. (slots sl[])
+// after their fetch has landed and a barrier: the MatShell apply's column
+// rule.  One thread per staged mask word; it visits only the word's set bits,
+// so rows without Dirichlet dofs cost one shared load.
+template <typename T, int TX, int NP>
+__device__ __forceinline__ void mask_planes(T *ut, const uint32_t *mw, const StreamGrid &g, int ex0, int ej, int64_t P0,
+                                            const int *sl)
+{
+  using L = TileLayout<TX>;
+  constexpr int RW = mask_row_words<TX>();
+  const int nd = 3 * min(L::NXN, 2 * (g.b.mx - ex0) + 1);
+  for (int j = threadIdx.x; j < NP * 3 * RW; j += TX) {
+    const int p = j / (3 * RW), r = (j / RW) % 3, w = j % RW;
+    uint32_t bits = mw[(sl[p] * 3 + r) * RW + w];
+    if (!bits) continue;
+    const int b0 = (int)((3 * row_node0(g, ex0, ej, r, P0 + p)) & 31);
+    while (bits) {
+      const int b = __ffs(bits) - 1;
+      bits &= bits - 1;
+      const int d = 32 * w + b - b0;
+      if (d >= 0 && d < nd) {
+        const int n = d / 3, c = d - 3 * n;
+        ut[L::at(c, sl[p], r, n)] = T(0);
+      }
+    }
+  }
+}
+
+// L2 prefetch (TMA unit, no registers) of the u rows of node plane P, each
+// row segment rounded out to 16-byte boundaries inside the array of nu values.
+template <typename T, int TX>
+__device__ __forceinline__ void prefetch_u_plane(const StreamGrid &g, int ex0, int ej, int64_t P, const T *u,
+                                                 int64_t nu)
+{
+  using L = TileLayout<TX>;
+  const int nd = 3 * min(L::NXN, 2 * (g.b.mx - ex0) + 1);
+  for (int r = 0; r < 3; r++) {
+    const int64_t k0 = 3 * row_node0(g, ex0, ej, r, P);
+    const uintptr_t a = (uintptr_t)(u + k0) & ~(uintptr_t)15;
+    const uintptr_t e = (uintptr_t)(u + min(k0 + nd, nu)) & ~(uintptr_t)15;
+    if (e > a) asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(a), "r"((uint32_t)(e - a)) : "memory");
   }
 }
 
@@ -168,12 +249,16 @@ __device__ __forceinline__ void zero_slot(T *yt, T *side, int s)
   }
 }
 
-// Flush node plane P (in slot s) to global y.  zlo/zhi: plane is the chunk's
-// first/last plane and shared with a neighbouring chunk.
-template <typename T, int TX, bool MASKED>
+// Flush node plane P (in slot s) to global y.  zshared: the plane is the
+// chunk's first/last plane and shared with a neighbouring chunk.  A node on a
+// tile boundary is stored by the first colour that touches it and added to
+// by the later ones; the colours are separate launches in a fixed order and
+// a launch touches each node from one CTA only, so the adds (red.global.add,
+// no read-back) happen in a fixed order: the sums are deterministic and equal
+// to a read-modify-write.  Dirichlet rows are set after the colour passes.
+template <typename T, int TX>
 __device__ __forceinline__ void flush_plane(const T *yt, const T *side, const StreamGrid &g, int tx, int ex0, int ej,
-                                            int64_t P, int s, bool zshared, T *__restrict__ y, const T *__restrict__ x,
-                                            const uint8_t *__restrict__ mask)
+                                            int64_t P, int s, bool zshared, T *__restrict__ y)
 {
   using L = TileLayout<TX>;
   const int nvalid = min(L::NXN, 2 * (g.b.mx - ex0) + 1);
@@ -182,22 +267,17 @@ __device__ __forceinline__ void flush_plane(const T *yt, const T *side, const St
   const int nd = 3 * nvalid;
 #pragma unroll 1
   for (int r = 0; r < 3; r++) {
-    const int64_t node0 = g.b.off + 2 * (int64_t)ex0 + (2 * (int64_t)ej + r) * g.b.X + P * g.b.XY;
+    const int64_t node0 = row_node0(g, ex0, ej, r, P);
     const bool yb = (r == 0 && ylo) || (r == 2 && yhi);
     for (int d = threadIdx.x; d < nd; d += TX) {
       const int n = d / 3, c = d - 3 * n;
       T v = yt[L::at(c, s, r, n)];
       if (L::NW > 1 && (n & 63) == 0 && n > 0 && n < 2 * TX) v += side[((n >> 6) - 1) * 27 + s * 9 + r * 3 + c];
       const int64_t k = 3 * node0 + d;
-      if (MASKED && mask[k]) {
-        y[k] = x[k];
-        continue;
-      }
       const bool xb = (n == 0 && xlo) || (n == 2 * TX && xhi);
-      // stored by the first colour touching the node, added by the later ones
       const bool first = !((xb && g.px) || (yb && g.py) || (zshared && g.pz));
       if (first) y[k] = v;
-      else y[k] = y[k] + v;
+      else atomicAdd(&y[k], v);
     }
   }
 }
@@ -274,9 +354,11 @@ __device__ __forceinline__ void element_plane(const T *ut, T *yt, T *side, const
 // The apply kernel
 // ---------------------------------------------------------------------------
 // One tile (x-tile tx, row ej, z-chunk zc) of one problem; the whole CTA.
+// MASKED (and mbits non-null): Dirichlet columns of u zeroed from the packed
+// mask mbits.
 template <typename T, int TX, bool MASKED>
 __device__ __forceinline__ void stream_tile(const StreamGrid &g, int tx, int ej, int zc, const T *__restrict__ K,
-                                            const T *__restrict__ u, const uint8_t *__restrict__ mask,
+                                            const T *__restrict__ u, const uint32_t *__restrict__ mbits,
                                             T *__restrict__ y)
 {
   using L = TileLayout<TX>;
@@ -284,20 +366,31 @@ __device__ __forceinline__ void stream_tile(const StreamGrid &g, int tx, int ej,
   T *ut = reinterpret_cast<T *>(smem_raw);
   T *yt = ut + L::TILE;
   T *side = yt + L::TILE;
+  uint32_t *mw = reinterpret_cast<uint32_t *>(side + L::SIDE);
   const int ex0 = tx * TX;
   const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
   const int ex = ex0 + t;
   const bool active = ex < g.b.mx;
   const int ek0 = zc * g.LZ, ek1 = min(ek0 + g.LZ, g.b.mz);
   const bool zlo_shared = zc > 0, zhi_shared = ek1 < g.b.mz;
+  // u holds at least the node planes up to the element box's last one
+  const int64_t nu = 3 * g.b.XY * (int64_t)(g.b.off / g.b.XY + 2 * (int64_t)g.b.mz + 1);
 
   // prologue: planes 2ek0 .. 2ek0+2 of u, zero y slots
   for (int k = 0; k < 3; k++) {
     const int64_t P = 2 * (int64_t)ek0 + k;
-    load_plane<T, TX, MASKED>(ut, g, ex0, ej, P, (int)(P % 3), u, mask);
-    zero_slot<T, TX>(yt, side, (int)(P % 3));
+    fetch_plane<T, TX, MASKED>(ut, mw, g, ex0, ej, P, (int)(P % 3), u, mbits);
   }
+  fetch_commit();
+  for (int k = 0; k < 3; k++) zero_slot<T, TX>(yt, side, (int)((2 * (int64_t)ek0 + k) % 3));
+  fetch_wait();
   __syncthreads();
+  if (MASKED && mbits) {
+    const int sl0[3] = {(int)((2 * (int64_t)ek0) % 3), (int)((2 * (int64_t)ek0 + 1) % 3),
+                        (int)((2 * (int64_t)ek0 + 2) % 3)};
+    mask_planes<T, TX, 3>(ut, mw, g, ex0, ej, 2 * (int64_t)ek0, sl0);
+    __syncthreads();
+  }
 
   // the node column of a thread's i=2 nodes lives in the side buffer for
   // lane 31 of every warp but the last
@@ -310,6 +403,12 @@ __device__ __forceinline__ void stream_tile(const StreamGrid &g, int tx, int ej,
     const int64_t row = ej + (int64_t)g.b.my * ek;
     const int s0 = (int)((2 * (int64_t)ek) % 3), s1 = (s0 + 1) % 3, s2 = (s0 + 2) % 3;
     const int sl[3] = {s0, s1, s2};
+    const bool more = ek + 1 < ek1;
+    // the next layer's two new node planes go to L2 while this one computes
+    if (t == 32 && more) {
+      prefetch_u_plane<T, TX>(g, ex0, ej, 2 * (int64_t)ek + 3, u, nu);
+      prefetch_u_plane<T, TX>(g, ex0, ej, 2 * (int64_t)ek + 4, u, nu);
+    }
 
     if (active) {
       // each quadrature plane's K is prefetched to L2 while the one before it computes
@@ -319,24 +418,31 @@ __device__ __forceinline__ void stream_tile(const StreamGrid &g, int tx, int ej,
       element_plane<T, TX, 0>(ut, yt, side, sl, t, warp, to_side, amask, K + krow, g.MXP);
       if (t == 0) prefetch_k_plane(K + kidx(row, 18, 0, g.MXP, 0), kb);
       element_plane<T, TX, 1>(ut, yt, side, sl, t, warp, to_side, amask, K + krow, g.MXP);
-      if (t == 0 && ek + 1 < ek1) prefetch_k_plane(K + kidx(row + g.b.my, 0, 0, g.MXP, 0), kb);
+      if (t == 0 && more) prefetch_k_plane(K + kidx(row + g.b.my, 0, 0, g.MXP, 0), kb);
       element_plane<T, TX, 2>(ut, yt, side, sl, t, warp, to_side, amask, K + krow, g.MXP);
     }
     __syncthreads();
 
-    // planes 2ek and 2ek+1 are complete for this CTA
-    flush_plane<T, TX, MASKED>(yt, side, g, tx, ex0, ej, 2 * (int64_t)ek, s0, ek == ek0 && zlo_shared, y, u, mask);
-    flush_plane<T, TX, MASKED>(yt, side, g, tx, ex0, ej, 2 * (int64_t)ek + 1, s1, false, y, u, mask);
-    if (ek + 1 == ek1)
-      flush_plane<T, TX, MASKED>(yt, side, g, tx, ex0, ej, 2 * (int64_t)ek + 2, s2, zhi_shared, y, u, mask);
-    __syncthreads();
-    if (ek + 1 < ek1) {
-      // slots s0, s1 take node planes 2ek+3, 2ek+4
+    // u slots s0, s1 are free: node planes 2ek+3, 2ek+4 land there while
+    // planes 2ek and 2ek+1 (complete for this CTA) are flushed
+    if (more) {
+      fetch_plane<T, TX, MASKED>(ut, mw, g, ex0, ej, 2 * (int64_t)ek + 3, s0, u, mbits);
+      fetch_plane<T, TX, MASKED>(ut, mw, g, ex0, ej, 2 * (int64_t)ek + 4, s1, u, mbits);
+      fetch_commit();
+    }
+    flush_plane<T, TX>(yt, side, g, tx, ex0, ej, 2 * (int64_t)ek, s0, ek == ek0 && zlo_shared, y);
+    flush_plane<T, TX>(yt, side, g, tx, ex0, ej, 2 * (int64_t)ek + 1, s1, false, y);
+    if (!more) flush_plane<T, TX>(yt, side, g, tx, ex0, ej, 2 * (int64_t)ek + 2, s2, zhi_shared, y);
+    if (more) {
+      __syncthreads();  // the flush has read y slots s0, s1
       zero_slot<T, TX>(yt, side, s0);
       zero_slot<T, TX>(yt, side, s1);
-      load_plane<T, TX, MASKED>(ut, g, ex0, ej, 2 * (int64_t)ek + 3, s0, u, mask);
-      load_plane<T, TX, MASKED>(ut, g, ex0, ej, 2 * (int64_t)ek + 4, s1, u, mask);
+      fetch_wait();
       __syncthreads();
+      if (MASKED && mbits) {
+        mask_planes<T, TX, 2>(ut, mw, g, ex0, ej, 2 * (int64_t)ek + 3, sl);
+        __syncthreads();
+      }
     }
   }
 }
@@ -355,13 +461,13 @@ constexpr int stream_min_blocks()
 template <typename T, int TX, bool MASKED>
 __global__ void __launch_bounds__(TX, stream_min_blocks<T, TX>()) a11_stream_kernel(StreamGrid g, const T *__restrict__ K,
                                                                   const T *__restrict__ u,
-                                                                  const uint8_t *__restrict__ mask,
+                                                                  const uint32_t *__restrict__ mbits,
                                                                   T *__restrict__ y)
 {
   // tile of this CTA within the colour class
   const int bid = blockIdx.x;
   const int ixc = bid % g.nxc, iyc = (bid / g.nxc) % g.nyc, izc = bid / (g.nxc * g.nyc);
-  stream_tile<T, TX, MASKED>(g, g.px + 2 * ixc, g.py + 2 * iyc, g.zc0 + 2 * izc, K, u, mask, y);
+  stream_tile<T, TX, MASKED>(g, g.px + 2 * ixc, g.py + 2 * iyc, g.zc0 + 2 * izc, K, u, mbits, y);
 }
 
 // ---------------------------------------------------------------------------
@@ -376,6 +482,8 @@ struct BatchProb {
   int64_t MXP;
   const void *K;          // T* of the problem's Gauss-point factor
   const uint8_t *mask;    // Dirichlet mask (MatShell level) or null
+  const uint32_t *mbits;  // the same mask packed one bit per dof
+  int64_t nvel;           // length of the problem's vectors
 };
 
 template <typename T, int TX, bool MASKED>
@@ -393,7 +501,7 @@ __global__ void __launch_bounds__(TX, stream_min_blocks<T, TX>()) a11_stream_bat
   g.nxc = g.nyc = g.nzcc = 0;
   g.zc0 = pz;
   stream_tile<T, TX, MASKED>(g, it.y, it.z, it.w, reinterpret_cast<const T *>(p.K), uptr[it.x],
-                             MASKED ? p.mask : nullptr, yptr[it.x]);
+                             MASKED ? p.mbits : nullptr, yptr[it.x]);
 }
 
 }  // namespace ptk

@@ -22,7 +22,6 @@
 #include "pt_b200.h"
 #include "kernels_colour.cuh"
 #include "kernels_stream.cuh"
-#include "kernels_tmem.cuh"
 #include "kernels_ebe.cuh"
 #include "kernels_markers.cuh"
 #include "kernels_bmat.cuh"
@@ -62,7 +61,7 @@ pt_status fail(pt_status s, const char *fmt, ...)
                   __LINE__);                                                                       \
   } while (0)
 
-enum A11Kernel { A11_STREAM = 0, A11_COLOUR = 1, A11_TMEM = 2, A11_EBE = 3 };
+enum A11Kernel { A11_STREAM = 0, A11_COLOUR = 1, A11_EBE = 3 };
 
 // "b200" picks stored element matrices for one-rank boxes up to this many
 // elements (packed FP64 + FP32 matrices: 40 KB per element, 1.3 GB at 32^3)
@@ -82,8 +81,9 @@ struct pt_op {
   double *d_coords, *d_eta;
   float *d_coords32, *d_eta32;
   uint8_t *d_mask;
+  uint32_t *d_mbits;  // the mask packed one bit per dof (the streaming kernel's column rule)
   bool has_coords, has_eta, has_mask;
-  double *d_u, *d_y, *d_p; // staging for _h calls
+  double *d_u, *d_y, *d_p, *d_yp; // staging for _h calls
   // streaming kernel: per-Gauss-point geometry K (FP64 and FP32 copies)
   double *d_K;
   float *d_K32;
@@ -109,6 +109,12 @@ struct pt_op {
   cudaStream_t h2d, d2h;
   cudaEvent_t ev_in[16], ev_done[16];
   bool pipe_ready;
+  // strided viscosity uploads: two pinned chunks and their copy events (first use)
+  double *h_stage[2];
+  cudaEvent_t ev_stage[2];
+  // momentum residual: Gauss-point body force [27 nel][3] and its load vector
+  double *d_fu, *d_F;
+  bool has_fu, F_valid;
 };
 
 namespace {
@@ -149,6 +155,41 @@ __global__ void bc_value_kernel(const uint8_t *__restrict__ mask, double v, doub
 {
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
     if (mask[i]) y[i] = v;
+}
+
+__global__ void sub_kernel(const double *__restrict__ a, double *__restrict__ y, int64_t n)
+{
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    y[i] -= a[i];
+}
+
+// y_k = x_k on the Dirichlet dofs, from the packed mask (one thread per word,
+// set bits only): the MatShell rows of the streaming apply.
+template <typename T>
+__global__ void bc_bits_kernel(const uint32_t *__restrict__ bits, const T *__restrict__ x, T *__restrict__ y, int64_t n)
+{
+  const int64_t nw = (n + 31) / 32;
+  for (int64_t w = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; w < nw; w += (int64_t)gridDim.x * blockDim.x) {
+    uint32_t b = bits[w];
+    while (b) {
+      const int j = __ffs(b) - 1;
+      b &= b - 1;
+      const int64_t k = 32 * w + j;
+      y[k] = x[k];
+    }
+  }
+}
+
+// bits[w] bit j = mask[32w + j] != 0 (one warp per word)
+__global__ void pack_mask_kernel(const uint8_t *__restrict__ mask, uint32_t *__restrict__ bits, int64_t n)
+{
+  const int64_t nw = (n + 31) / 32;
+  const int64_t wpb = blockDim.x / 32;
+  for (int64_t w = (int64_t)blockIdx.x * wpb + threadIdx.x / 32; w < nw; w += (int64_t)gridDim.x * wpb) {
+    const int64_t i = 32 * w + (threadIdx.x & 31);
+    const unsigned b = __ballot_sync(0xffffffffu, i < n && mask[i]);
+    if ((threadIdx.x & 31) == 0) bits[w] = b;
+  }
 }
 
 unsigned grid_stride_blocks(int64_t n)
@@ -232,6 +273,7 @@ template <typename T, int TX, bool MASKED>
 pt_status launch_stream_tx(pt_op *op, const T *K, const T *u, T *y, int zb = 0, int ze = -1)
 {
   if (ze < 0) ze = op->nzc;
+  if (MASKED && !op->d_mbits) return fail(PT_ERR_STATE, "masked apply without the packed Dirichlet bits");
   constexpr size_t smem = ptk::stream_smem_bytes<T, TX>();
   pt_status as = kernel_attrs((const void *)ptk::a11_stream_kernel<T, TX, MASKED>, smem);
   if (as != PT_OK) return as;
@@ -248,39 +290,11 @@ pt_status launch_stream_tx(pt_op *op, const T *K, const T *u, T *y, int zb = 0, 
         g.nzcc = g.zc0 < ze ? (ze - g.zc0 + 1) / 2 : 0;
         const int64_t n = (int64_t)g.nxc * g.nyc * g.nzcc;
         if (n == 0) continue;
-        ptk::a11_stream_kernel<T, TX, MASKED><<<(unsigned)n, TX, smem, op->stream>>>(g, K, u, MASKED ? op->d_mask : nullptr, y);
+        ptk::a11_stream_kernel<T, TX, MASKED><<<(unsigned)n, TX, smem, op->stream>>>(g, K, u, MASKED ? op->d_mbits : nullptr, y);
         PT_LAUNCHED(op);
       }
   return PT_OK;
 }
-
-template <bool MASKED>
-pt_status launch_tmem(pt_op *op, const double *K, const double *u, double *y)
-{
-  constexpr size_t smem = ptk::tmem_smem_bytes();
-  pt_status as = kernel_attrs((const void *)ptk::a11_tmem_kernel<MASKED>, smem, false);
-  if (as != PT_OK) return as;
-  ptk::StreamGrid g;
-  g.b = op->box;
-  g.TX = 128; g.ntx = op->ntx; g.LZ = op->LZ; g.nzc = op->nzc; g.MXP = op->MXP;
-  for (int pz = 0; pz < 2; pz++)
-    for (int py = 0; py < 2; py++)
-      for (int px = 0; px < 2; px++) {
-        g.px = px; g.py = py; g.pz = pz;
-        g.nxc = (op->ntx - px + 1) / 2;
-        g.nyc = (op->my - py + 1) / 2;
-        g.nzcc = (op->nzc - pz + 1) / 2;
-        g.zc0 = pz;
-        const int64_t n = (int64_t)g.nxc * g.nyc * g.nzcc;
-        if (n == 0) continue;
-        ptk::a11_tmem_kernel<MASKED><<<(unsigned)n, 128, smem, op->stream>>>(g, K, u, MASKED ? op->d_mask : nullptr, y);
-        PT_LAUNCHED(op);
-      }
-  return PT_OK;
-}
-
-template <typename T, bool MASKED>
-pt_status launch_stream_any(pt_op *op, const T *K, const T *u, T *y);
 
 template <typename T, bool MASKED>
 pt_status launch_stream(pt_op *op, const T *K, const T *u, T *y)
@@ -288,18 +302,6 @@ pt_status launch_stream(pt_op *op, const T *K, const T *u, T *y)
   if (op->TX == 32) return launch_stream_tx<T, 32, MASKED>(op, K, u, y);
   if (op->TX == 64) return launch_stream_tx<T, 64, MASKED>(op, K, u, y);
   return launch_stream_tx<T, 128, MASKED>(op, K, u, y);
-}
-
-// "b200": the shared-memory streaming kernel; "b200_tmem": its variant with
-// TMEM accumulators and a cp.async K ring, for FP64 rows of 65..128 elements
-// (measured slower at 128^3: 5.5 ms vs 4.0 ms per apply).
-template <typename T, bool MASKED>
-pt_status launch_stream_any(pt_op *op, const T *K, const T *u, T *y)
-{
-  if constexpr (std::is_same<T, double>::value) {
-    if (op->a11_kernel == A11_TMEM && op->TX == 128) return launch_tmem<MASKED>(op, K, u, y);
-  }
-  return launch_stream<T, MASKED>(op, K, u, y);
 }
 
 // Recompute K when coordinates or viscosity changed.  Sets geom_ok = false
@@ -384,11 +386,11 @@ pt_status launch_ebe(pt_op *op, const T *u, T *y, bool masked)
 
 // ---- A11 dispatch -----------------------------------------------------------
 
-// The streaming kernels write y_k = x_k on Dirichlet dofs themselves (and
-// launch_a11 does it for ghost nodes), so MatMult needs no separate pass.
+// The streaming and stored-matrix applies set y_k = x_k on Dirichlet dofs
+// inside launch_a11, so MatMult needs no separate pass after them.
 bool a11_sets_bc_rows(const pt_op *op)
 {
-  const bool stream = op->a11_kernel == A11_STREAM || op->a11_kernel == A11_TMEM;
+  const bool stream = op->a11_kernel == A11_STREAM;
   const bool ebe = op->a11_kernel == A11_EBE && op->full_box;
   return (stream || ebe) && op->geom_ok && !op->geom_dirty;
 }
@@ -408,22 +410,19 @@ pt_status launch_a11(pt_op *op, const T *coords, const T *eta, const T *u, T *y,
     if (s != PT_OK) return s;
     if (op->geom_ok) return launch_ebe<T>(op, u, y, masked);
   }
-  if (op->a11_kernel == A11_STREAM || op->a11_kernel == A11_TMEM) {
+  if (op->a11_kernel == A11_STREAM) {
     pt_status s = ensure_geometry(op);
     if (s != PT_OK) return s;
     if (op->geom_ok) {
       if (!op->full_box) PT_CUDA(cudaMemsetAsync(y, 0, sizeof(T) * op->nvel, op->stream));
       if (masked) {
-        if ((s = launch_stream_any<T, true>(op, op_K<T>(op), u, y)) != PT_OK) return s;
-        // the kernel writes y_k = x_k on Dirichlet dofs inside the element box;
-        // nodes outside it (ghost layers) get the same rule here
-        if (!op->full_box) {
-          bc_copy_kernel<T><<<grid_stride_blocks(op->nvel), 256, 0, op->stream>>>(op->d_mask, u, y, op->nvel);
-          PT_LAUNCHED(op);
-        }
+        // Dirichlet columns inside the kernel; rows y_k = x_k after its colour passes
+        if ((s = launch_stream<T, true>(op, op_K<T>(op), u, y)) != PT_OK) return s;
+        bc_bits_kernel<T><<<grid_stride_blocks((op->nvel + 31) / 32), 256, 0, op->stream>>>(op->d_mbits, u, y, op->nvel);
+        PT_LAUNCHED(op);
         return PT_OK;
       }
-      return launch_stream_any<T, false>(op, op_K<T>(op), u, y);
+      return launch_stream<T, false>(op, op_K<T>(op), u, y);
     }
   }
   PT_CUDA(cudaMemsetAsync(y, 0, sizeof(T) * op->nvel, op->stream));
@@ -631,6 +630,12 @@ pt_status a11_host_pipelined(pt_op *op, const double *hu, double *hy, bool *done
     if (s != PT_OK) return s;
     PT_CUDA(cudaEventRecord(op->ev_done[gi], op->stream));
     const int64_t fin = last ? nplanes : top;  // planes below `fin` are final
+    if (MASKED && fin > down) {  // their Dirichlet rows, y_k = x_k
+      const int64_t o = down * plane, m = (fin - down) * plane;
+      bc_copy_kernel<double><<<grid_stride_blocks(m), 256, 0, op->stream>>>(op->d_mask + o, op->d_u + o, op->d_y + o, m);
+      PT_LAUNCHED(op);
+      PT_CUDA(cudaEventRecord(op->ev_done[gi], op->stream));
+    }
     if (fin > down) {
       PT_CUDA(cudaStreamWaitEvent(op->d2h, op->ev_done[gi], 0));
       PT_CUDA(cudaMemcpyAsync(hy + down * plane, op->d_y + down * plane, sizeof(double) * (fin - down) * plane,
@@ -720,8 +725,14 @@ pt_status pt_op_destroy(pt_op *op)
   if (op->stream && !op->pool) cudaStreamSynchronize(op->stream);
   void *bufs[] = {op->d_coords, op->d_eta, op->d_coords32, op->d_eta32, op->d_mask, op->d_u,
                   op->d_y, op->d_p, op->d_K, op->d_K32, op->d_bad, op->d_Ae, op->d_Ae32, op->d_ye,
-                  op->mk_scratch, op->d_Be};
+                  op->mk_scratch, op->d_Be, op->d_yp, op->d_mbits, op->d_fu, op->d_F};
   for (void *b : bufs) op_free(op, b);
+  for (int b = 0; b < 2; b++)
+    if (op->h_stage[b]) {
+      cudaEventSynchronize(op->ev_stage[b]);
+      cudaEventDestroy(op->ev_stage[b]);
+      cudaFreeHost(op->h_stage[b]);
+    }
   if (op->own_stream && op->stream) cudaStreamDestroy(op->stream);
   if (op->pipe_ready) {
     cudaStreamSynchronize(op->h2d);
@@ -763,6 +774,7 @@ static pt_status finish_coords(pt_op *op)
   op->has_coords = true;
   op->geom_dirty = true;
   op->be_valid = false;
+  op->F_valid = false;
   op->state++;
   return PT_OK;
 }
@@ -811,18 +823,49 @@ pt_status pt_op_set_eta_d(pt_op *op, const double *eta)
   return finish_eta(op);
 }
 
+// Gathers eta0[i*stride] (the eta member of an array of QPntVolCoefStokes
+// records) through two op-owned pinned chunks: while one chunk's copy runs on
+// the op's stream the host fills the other.  The chunks are allocated once.
+constexpr int64_t ETA_STAGE_DOUBLES = (int64_t)1 << 19;  // 4 MiB per chunk
+
 pt_status pt_op_set_eta_strided_h(pt_op *op, const double *eta0, int64_t stride)
 {
   if (!op || !eta0) return fail(PT_ERR_BAD_ARG, "NULL argument");
   if (stride < 1) return fail(PT_ERR_BAD_ARG, "stride must be >= 1 (got %lld)", (long long)stride);
   if (stride == 1) return pt_op_set_eta_h(op, eta0);
+  if (!op->h_stage[0]) {
+    for (int b = 0; b < 2; b++) {
+      PT_CUDA(cudaMallocHost(&op->h_stage[b], sizeof(double) * ETA_STAGE_DOUBLES));
+      PT_CUDA(cudaEventCreateWithFlags(&op->ev_stage[b], cudaEventDisableTiming));
+    }
+  }
   const int64_t n = 27 * op->nel;
-  double *tmp = nullptr;
-  PT_CUDA(cudaMallocHost(&tmp, sizeof(double) * n));
-  for (int64_t i = 0; i < n; i++) tmp[i] = eta0[i * stride];
-  pt_status s = pt_op_set_eta_h(op, tmp);
-  cudaFreeHost(tmp);
-  return s;
+  for (int64_t c0 = 0, k = 0; c0 < n; c0 += ETA_STAGE_DOUBLES, k++) {
+    const int b = (int)(k & 1);
+    const int64_t m = std::min(ETA_STAGE_DOUBLES, n - c0);
+    PT_CUDA(cudaEventSynchronize(op->ev_stage[b]));  // the copy that last read this chunk is done
+    double *dst = op->h_stage[b];
+    const double *src = eta0 + c0 * stride;
+    for (int64_t i = 0; i < m; i++) dst[i] = src[i * stride];
+    PT_CUDA(cudaMemcpyAsync(op->d_eta + c0, dst, sizeof(double) * m, cudaMemcpyHostToDevice, op->stream));
+    PT_CUDA(cudaEventRecord(op->ev_stage[b], op->stream));
+  }
+  pt_status s = finish_eta(op);
+  if (s != PT_OK) return s;
+  PT_CUDA(cudaStreamSynchronize(op->stream));
+  return PT_OK;
+}
+
+// After d_mask changed: its packed bits (allocated on first use), on the op's stream.
+static pt_status finish_mask(pt_op *op)
+{
+  const int64_t nw = (op->nvel + 31) / 32;
+  if (!op->d_mbits) PT_CUDA(op_alloc(op, (void **)&op->d_mbits, sizeof(uint32_t) * nw));
+  pack_mask_kernel<<<grid_stride_blocks(32 * nw), 256, 0, op->stream>>>(op->d_mask, op->d_mbits, op->nvel);
+  PT_LAUNCHED(op);
+  op->has_mask = true;
+  op->state++;
+  return PT_OK;
 }
 
 pt_status pt_op_set_bc_mask_h(pt_op *op, const uint8_t *mask)
@@ -834,8 +877,8 @@ pt_status pt_op_set_bc_mask_h(pt_op *op, const uint8_t *mask)
     op->state++;
   } else {
     PT_CUDA(cudaMemcpyAsync(op->d_mask, mask, op->nvel, cudaMemcpyHostToDevice, op->stream));
-    op->has_mask = true;
-    op->state++;
+    pt_status s = finish_mask(op);
+    if (s != PT_OK) return s;
   }
   PT_CUDA(cudaStreamSynchronize(op->stream));
   return PT_OK;
@@ -846,6 +889,7 @@ static pt_status ensure_staging(pt_op *op)
   if (!op->d_u) PT_CUDA(op_alloc(op, (void **)&op->d_u, sizeof(double) * op->nvel));
   if (!op->d_y) PT_CUDA(op_alloc(op, (void **)&op->d_y, sizeof(double) * op->nvel));
   if (!op->d_p) PT_CUDA(op_alloc(op, (void **)&op->d_p, sizeof(double) * op->npres));
+  if (!op->d_yp) PT_CUDA(op_alloc(op, (void **)&op->d_yp, sizeof(double) * op->npres));
   return PT_OK;
 }
 
@@ -1041,8 +1085,7 @@ static pt_status stokes_host(pt_op *op, const double *u, const double *p, double
   if (s != PT_OK) return s;
   if (!u || !p || !yu || !yp) return fail(PT_ERR_BAD_ARG, "NULL vector");
   if ((s = ensure_staging(op)) != PT_OK) return s;
-  double *dyp = nullptr;
-  PT_CUDA(op_alloc(op, (void **)&dyp, sizeof(double) * op->npres));
+  double *dyp = op->d_yp;
   cudaError_t e = cudaMemcpyAsync(op->d_u, u, sizeof(double) * op->nvel, cudaMemcpyHostToDevice, op->stream);
   if (e == cudaSuccess) e = cudaMemcpyAsync(op->d_p, p, sizeof(double) * op->npres, cudaMemcpyHostToDevice, op->stream);
   if (e == cudaSuccess) {
@@ -1052,7 +1095,6 @@ static pt_status stokes_host(pt_op *op, const double *u, const double *p, double
       e = cudaMemcpyAsync(yp, dyp, sizeof(double) * op->npres, cudaMemcpyDeviceToHost, op->stream);
     if (s == PT_OK && e == cudaSuccess) e = cudaStreamSynchronize(op->stream);
   }
-  op_free(op, dyp);
   if (s != PT_OK) return s;
   if (e != cudaSuccess) return fail(PT_ERR_CUDA, "Stokes operator host call: %s", cudaGetErrorString(e));
   return PT_OK;
@@ -1066,6 +1108,95 @@ pt_status pt_stokes_a_apply_h(pt_op *op, const double *u, const double *p, doubl
 pt_status pt_matmult_a_h(pt_op *op, const double *xu, const double *xp, double *yu, double *yp)
 {
   return stokes_host(op, xu, xp, yu, yp, true);
+}
+
+// ---- momentum residual (FormFunctionLocal_U) ---------------------------------
+
+static pt_status fu_alloc(pt_op *op)
+{
+  if (!op->d_fu) PT_CUDA(op_alloc(op, (void **)&op->d_fu, sizeof(double) * 3 * 27 * op->nel));
+  return PT_OK;
+}
+
+pt_status pt_op_set_body_force_h(pt_op *op, const double *fu)
+{
+  if (!op || !fu) return fail(PT_ERR_BAD_ARG, "NULL argument");
+  pt_status s = fu_alloc(op);
+  if (s != PT_OK) return s;
+  PT_CUDA(cudaMemcpyAsync(op->d_fu, fu, sizeof(double) * 3 * 27 * op->nel, cudaMemcpyHostToDevice, op->stream));
+  PT_CUDA(cudaStreamSynchronize(op->stream));
+  op->has_fu = true;
+  op->F_valid = false;
+  return PT_OK;
+}
+
+pt_status pt_op_set_body_force_d(pt_op *op, const double *fu)
+{
+  if (!op || !fu) return fail(PT_ERR_BAD_ARG, "NULL argument");
+  pt_status s = fu_alloc(op);
+  if (s != PT_OK) return s;
+  PT_CUDA(cudaMemcpyAsync(op->d_fu, fu, sizeof(double) * 3 * 27 * op->nel, cudaMemcpyDeviceToDevice, op->stream));
+  op->has_fu = true;
+  op->F_valid = false;
+  return PT_OK;
+}
+
+pt_status pt_op_set_body_force_strided_h(pt_op *op, const double *fu0, int64_t stride)
+{
+  if (!op || !fu0) return fail(PT_ERR_BAD_ARG, "NULL argument");
+  if (stride < 3) return fail(PT_ERR_BAD_ARG, "stride must be >= 3 (got %lld)", (long long)stride);
+  const int64_t nq = 27 * op->nel;
+  std::vector<double> tmp((size_t)(3 * nq));
+  for (int64_t i = 0; i < nq; i++)
+    for (int c = 0; c < 3; c++) tmp[(size_t)(3 * i + c)] = fu0[i * stride + c];
+  return pt_op_set_body_force_h(op, tmp.data());
+}
+
+// F = the body-force load vector of the current coordinates and body force.
+static pt_status ensure_body_force(pt_op *op)
+{
+  if (op->F_valid) return PT_OK;
+  if (!op->d_F) PT_CUDA(op_alloc(op, (void **)&op->d_F, sizeof(double) * op->nvel));
+  PT_CUDA(cudaMemsetAsync(op->d_F, 0, sizeof(double) * op->nvel, op->stream));
+  for (int c = 0; c < 8; c++) {
+    ptk::ColourGrid g = ptk::colour_grid(op->box, c);
+    const int64_t n = (int64_t)g.ncx * g.ncy * g.ncz;
+    if (n == 0) continue;
+    ptk::body_force_colour_kernel<<<nblocks(n), TPB, 0, op->stream>>>(g, op->d_coords, op->d_fu, op->d_F);
+    PT_LAUNCHED(op);
+  }
+  op->F_valid = true;
+  return PT_OK;
+}
+
+pt_status pt_residual_u_d(pt_op *op, const double *u, const double *p, double *ru)
+{
+  pt_status s = check_ready(op, true);
+  if (s != PT_OK) return s;
+  if (!op->has_fu) return fail(PT_ERR_STATE, "body force not set (pt_op_set_body_force_*)");
+  if (!u || !p || !ru) return fail(PT_ERR_BAD_ARG, "NULL vector");
+  if (u == ru) return fail(PT_ERR_BAD_ARG, "u and ru must not alias");
+  // u as given (the caller inserted the Dirichlet values): no column rule
+  if ((s = launch_a11<double>(op, op->d_coords, op->d_eta, u, ru, false)) != PT_OK) return s;
+  if ((s = a12_d(op, p, ru, true)) != PT_OK) return s;
+  if ((s = ensure_body_force(op)) != PT_OK) return s;
+  sub_kernel<<<grid_stride_blocks(op->nvel), 256, 0, op->stream>>>(op->d_F, ru, op->nvel);
+  PT_LAUNCHED(op);
+  return PT_OK;
+}
+
+pt_status pt_residual_u_h(pt_op *op, const double *u, const double *p, double *ru)
+{
+  pt_status s = check_ready(op, true);
+  if (s != PT_OK) return s;
+  if (!u || !p || !ru) return fail(PT_ERR_BAD_ARG, "NULL vector");
+  if ((s = ensure_staging(op)) != PT_OK) return s;
+  PT_CUDA(cudaMemcpyAsync(op->d_u, u, sizeof(double) * op->nvel, cudaMemcpyHostToDevice, op->stream));
+  PT_CUDA(cudaMemcpyAsync(op->d_p, p, sizeof(double) * op->npres, cudaMemcpyHostToDevice, op->stream));
+  if ((s = pt_residual_u_d(op, op->d_u, op->d_p, op->d_y)) != PT_OK) return s;
+  PT_CUDA(cudaMemcpyAsync(ru, op->d_y, sizeof(double) * op->nvel, cudaMemcpyDeviceToHost, op->stream));
+  PT_CUDA(cudaStreamSynchronize(op->stream));
+  return PT_OK;
 }
 
 // ---- marker -> Gauss-point coefficients --------------------------------------
@@ -1187,7 +1318,6 @@ pt_status pt_op_set_a11_kernel(pt_op *op, const char *name)
   else if (!strcmp(name, "b200_stream")) op->a11_kernel = A11_STREAM;
   else if (!strcmp(name, "b200_ebe")) op->a11_kernel = A11_EBE;
   else if (!strcmp(name, "b200_colour")) op->a11_kernel = A11_COLOUR;
-  else if (!strcmp(name, "b200_tmem")) op->a11_kernel = A11_TMEM;
   else return fail(PT_ERR_BAD_ARG, "No -a11_op %s", name);
   return PT_OK;
 }
@@ -1215,7 +1345,6 @@ const char *pt_op_get_a11_kernel(const pt_op *op)
   if (!op) return "";
   switch (op->a11_kernel) {
     case A11_STREAM: return "b200_stream";
-    case A11_TMEM: return "b200_tmem";
     case A11_EBE: return "b200_ebe";
     default: return "b200_colour";
   }

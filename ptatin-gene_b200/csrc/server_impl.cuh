@@ -563,7 +563,7 @@ pt_status srv_admit(pt_server *s, SrvReq *r, int slot)
   if ((e = finish_eta(op)) != PT_OK) return e;
   if (r->h_mask) {
     PT_CUDA(cudaMemcpyAsync(op->d_mask, r->h_mask, n, cudaMemcpyHostToDevice, st));
-    op->has_mask = true;
+    if ((e = finish_mask(op)) != PT_OK) return e;
   }
   s->h_bad[slot] = 0;
   if ((e = srv_geometry(op, &s->h_bad[slot])) != PT_OK) return e;
@@ -721,14 +721,14 @@ pt_status srv_iterate(pt_server *s)
   void **tab = (void **)s->d_ptrs;
   pt_status e = batch_apply<double, true>(s->batch, (const double *const *)tab, (double *const *)(tab + n), st);
   if (e != PT_OK) return e;
-  s->launches += s->batch->classes.size();
+  s->launches += s->batch->classes.size() + 1;
   srv_pq_kernel<<<ni, SRV_THREADS, 0, st>>>(s->d_items, s->d_slots, s->d_scal);
   srv_final_kernel<SRV_F_ALPHA><<<na, SRV_THREADS, 0, st>>>(s->d_act, s->d_slots, s->d_scal);
   srv_update_kernel<<<ni, SRV_THREADS, 0, st>>>(s->d_items, s->d_slots, s->d_scal);
   srv_final_kernel<SRV_F_RR><<<na, SRV_THREADS, 0, st>>>(s->d_act, s->d_slots, s->d_scal);
   s->launches += 4;
   e = srv_precond<T>(s, s->d_items, ni, st, [&]() {
-    s->launches += s->batch->classes.size();
+    s->launches += s->batch->classes.size() + 1;
     return batch_apply<T, true>(s->batch, (const T *const *)(tab + 2 * n), (T *const *)(tab + 3 * n), st);
   });
   if (e != PT_OK) return e;

@@ -401,7 +401,7 @@ pt_status mg_coarsen(const pt_op *f, const double *vf_f, double *vf_c, pt_op **o
   if ((st = finish_eta(c)) != PT_OK) return st;
   inject_mask_kernel<<<vgrid(c->nnodes), 256, 0, c->stream>>>(fb, cb, f->d_mask, c->d_mask);
   PT_LAUNCHED(c);
-  c->has_mask = f->has_mask;
+  if (f->has_mask) return finish_mask(c);  // the packed bits the streaming kernel reads
   return PT_OK;
 }
 

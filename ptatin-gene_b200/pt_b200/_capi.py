@@ -92,6 +92,11 @@ SIGNATURES = {
     "pt_matmult_a21_d": [_vp, _vp, _vp],
     "pt_stokes_a_apply_d": [_vp, _vp, _vp, _vp, _vp],
     "pt_stokes_a_apply_h": [_vp, _vp, _vp, _vp, _vp],
+    "pt_op_set_body_force_h": [_vp, _vp],
+    "pt_op_set_body_force_d": [_vp, _vp],
+    "pt_op_set_body_force_strided_h": [_vp, _vp, ctypes.c_int64],
+    "pt_residual_u_d": [_vp, _vp, _vp, _vp],
+    "pt_residual_u_h": [_vp, _vp, _vp, _vp],
     "pt_matmult_a_d": [_vp, _vp, _vp, _vp, _vp],
     "pt_matmult_a_h": [_vp, _vp, _vp, _vp, _vp],
     "pt_project_markers_d": [_vp, ctypes.c_int64, _vp, _vp, _vp, _vp, _vp, _vp, ctypes.c_int],

@@ -29,7 +29,7 @@ try:  # torch is plumbing only (device memory, streams); optional on CPU hosts
 except Exception:  # pragma: no cover
     torch = None
 
-A11_OPS = ("b200", "b200_stream", "b200_ebe", "b200_tmem", "b200_colour")
+A11_OPS = ("b200", "b200_stream", "b200_ebe", "b200_colour")
 
 
 def _is_dev(a) -> bool:
@@ -268,6 +268,33 @@ class MatStokesMF:
         _capi.call("pt_project_markers_h", self._h, n, w.ctypes.data, x.ctypes.data, e.ctypes.data, r.ctypes.data,
                    eq.ctypes.data, rq.ctypes.data, int(install))
         return eq, rq
+
+    def set_body_force(self, fu):
+        """Gauss-point body force QPntVolCoefStokes.Fu, [27 nel][3] (numpy or
+        a CUDA float64 tensor)."""
+        self._check_len(fu, 3 * 27 * self.nel, "fu")
+        if _is_dev(fu):
+            _capi.call("pt_op_set_body_force_d", self._h, _dptr(fu, torch.float64))
+        else:
+            f = np.ascontiguousarray(fu, dtype=np.float64)
+            _capi.call("pt_op_set_body_force_h", self._h, _hptr(f, np.float64))
+
+    def FormFunctionLocal_U(self, ufield, pfield, Ru=None):
+        """The unassembled local momentum residual A11 u + A12 p - body force
+        (FormFunctionLocal_U, src/stokes_form_function.c:99-243); u as given,
+        with the Dirichlet values inserted by the caller."""
+        self._check_len(ufield, self.nvel, "u")
+        self._check_len(pfield, self.npres, "p")
+        if _is_dev(ufield):
+            Ru = torch.empty_like(ufield) if Ru is None else Ru
+            _capi.call("pt_residual_u_d", self._h, _dptr(ufield, torch.float64), _dptr(pfield, torch.float64),
+                       _dptr(Ru, torch.float64))
+            return Ru
+        u = np.ascontiguousarray(ufield, dtype=np.float64)
+        p = np.ascontiguousarray(pfield, dtype=np.float64)
+        Ru = np.empty(self.nvel) if Ru is None else Ru
+        _capi.call("pt_residual_u_h", self._h, _hptr(u, np.float64), _hptr(p, np.float64), _hptr(Ru, np.float64))
+        return Ru
 
     def MFStokesWrapper_A(self, ufield, pfield, Yu=None, Yp=None):
         """The whole Stokes operator, unassembled and without BCs:

@@ -16,11 +16,22 @@
  * ufield/Xp/Xu are the rank's ghosted local arrays (Dirichlet entries already
  * zeroed by the caller), the output array is the zeroed local vector that the
  * caller scatters with DMLocalToGlobal(ADD_VALUES) and then fixes the BC rows.
- * The back-end does no BC work.  Coordinates and quadrature-point viscosity
- * are uploaded when the Mat's PetscObjectState changes (mf->state), as the
- * reference CUDA back-end does (src/stokes_operators_cuda.cu:413-422), and
- * otherwise stay resident in HBM.  Errors come back as PetscErrorCode; the
+ * The back-end does no BC work.  Errors come back as PetscErrorCode; the
  * library never exits the process.
+ *
+ * Device data.  One pt_op per velocity DM holds the coordinates, the
+ * quadrature-point viscosity and everything derived from them (the Gauss-point
+ * geometry factors, the divergence blocks); the A11 shell (mf->ctx) and the
+ * diag / B / B^T / whole-operator calls all use it, so a run keeps one copy.
+ *   - coordinates are uploaded when the coordinate Vec (or its
+ *     PetscObjectState) changes, i.e. when the mesh moves;
+ *   - the viscosity is uploaded when the state of the calling Mat changes, as
+ *     the reference CUDA back-end does with mf->state
+ *     (src/stokes_operators_cuda.cu:413-422).  Each calling Mat (the A11 shell
+ *     for MatMult and MatGetDiagonal, the Stokes shell for the whole operator)
+ *     is tracked by its own last-seen state.
+ * Only an upload invalidates the derived data, so repeated MatMults with
+ * unchanged coordinates and viscosity run the kernels alone.
  *
  * Build (where PETSc and pTatin3D are available): compile this file with the
  * pTatin3D include path and -I<repo>/include, link -lpt_b200.
@@ -36,10 +47,25 @@
 
 #include "pt_b200.h"
 
+#define B200_ETA_KEYS 8
+
+/* The op shared by every caller on one velocity DM. */
 typedef struct {
   pt_op *op;
-  PetscObjectState state; /* state of the uploaded coordinates / viscosity */
-  PetscBool have_data;
+  Vec coords_vec;                 /* the coordinate Vec last uploaded ... */
+  PetscObjectState coords_state;  /* ... and its state then */
+  PetscBool have_coords, have_eta;
+  struct {
+    const void *key;              /* the calling Mat */
+    PetscObjectState state;       /* its state at the last viscosity upload it saw */
+  } eta_seen[B200_ETA_KEYS];
+  int n_seen, next_slot;
+} B200Op;
+
+/* mf->ctx of the A11 shell: a reference to the DM's op. */
+typedef struct {
+  PetscContainer cont;
+  B200Op *b;
 } MFA11B200;
 
 #define PTCHK(call)                                                                                 \
@@ -65,39 +91,104 @@ static PetscErrorCode B200_MeshDesc(DM dau, pt_mesh_desc *d)
   PetscFunctionReturn(0);
 }
 
-static PetscErrorCode B200_Create(DM dau, MFA11B200 **out)
+static PetscErrorCode B200_OpDestroy(void *ctx)
+{
+  B200Op *b = (B200Op *)ctx;
+  if (b) {
+    pt_op_destroy(b->op);
+    PetscFree(b);
+  }
+  return 0;
+}
+
+/* The op composed on dau ("pt_b200_op"), created on first use; the DM holds
+ * the only reference unless *cont_ref is asked for (then the caller owns one
+ * more and releases it with PetscContainerDestroy). */
+static PetscErrorCode B200_Shared(DM dau, B200Op **out, PetscContainer *cont_ref)
 {
   PetscErrorCode ierr;
-  pt_mesh_desc d;
-  MFA11B200 *c;
+  PetscContainer cont = NULL;
+  B200Op *b;
 
   PetscFunctionBegin;
-  ierr = B200_MeshDesc(dau, &d);CHKERRQ(ierr);
-  ierr = PetscCalloc1(1, &c);CHKERRQ(ierr);
-  PTCHK(pt_op_create(&d, &c->op));
-  c->state = -1;
-  *out = c;
+  ierr = PetscObjectQuery((PetscObject)dau, "pt_b200_op", (PetscObject *)&cont);CHKERRQ(ierr);
+  if (!cont) {
+    pt_mesh_desc d;
+    ierr = B200_MeshDesc(dau, &d);CHKERRQ(ierr);
+    ierr = PetscCalloc1(1, &b);CHKERRQ(ierr);
+    if (pt_op_create(&d, &b->op) != PT_OK) {
+      ierr = PetscFree(b);CHKERRQ(ierr);
+      SETERRQ1(PETSC_COMM_SELF, PETSC_ERR_LIB, "pt_op_create: %s", pt_last_error());
+    }
+    ierr = PetscContainerCreate(PetscObjectComm((PetscObject)dau), &cont);CHKERRQ(ierr);
+    ierr = PetscContainerSetPointer(cont, b);CHKERRQ(ierr);
+    ierr = PetscContainerSetUserDestroy(cont, B200_OpDestroy);CHKERRQ(ierr);
+    ierr = PetscObjectCompose((PetscObject)dau, "pt_b200_op", (PetscObject)cont);CHKERRQ(ierr);
+    ierr = PetscContainerDestroy(&cont);CHKERRQ(ierr);
+    ierr = PetscObjectQuery((PetscObject)dau, "pt_b200_op", (PetscObject *)&cont);CHKERRQ(ierr);
+  }
+  ierr = PetscContainerGetPointer(cont, (void **)&b);CHKERRQ(ierr);
+  if (cont_ref) {
+    ierr = PetscObjectReference((PetscObject)cont);CHKERRQ(ierr);
+    *cont_ref = cont;
+  }
+  *out = b;
   PetscFunctionReturn(0);
 }
 
-/* Upload coordinates and eta (QPntVolCoefStokes AoS, eta at offset 0). */
-static PetscErrorCode B200_Upload(MFA11B200 *c, Quadrature volQ, DM dau, PetscBool need_eta)
+/* Brings the op's coordinates (and, with need_eta, viscosity) up to date:
+ * coordinates when the coordinate Vec or its state changed, viscosity when the
+ * calling Mat `key` shows a state other than the one it showed at its last
+ * upload (or has never been seen).  QPntVolCoefStokes is a 48-byte record
+ * with eta at offset 0 (include/QPntVolCoefStokes_def.h:41-46). */
+static PetscErrorCode B200_Sync(B200Op *b, DM dau, Quadrature volQ, const void *key, PetscObjectState key_state,
+                                PetscBool need_eta)
 {
   PetscErrorCode ierr;
   Vec gcoords;
-  const PetscScalar *LA_gcoords;
-  QPntVolCoefStokes *qp;
+  PetscObjectState st;
 
   PetscFunctionBegin;
   ierr = DMGetCoordinatesLocal(dau, &gcoords);CHKERRQ(ierr);
-  ierr = VecGetArrayRead(gcoords, &LA_gcoords);CHKERRQ(ierr);
-  PTCHK(pt_op_set_coords_h(c->op, LA_gcoords));
-  ierr = VecRestoreArrayRead(gcoords, &LA_gcoords);CHKERRQ(ierr);
-  if (need_eta) {
-    ierr = VolumeQuadratureGetAllCellData_Stokes(volQ, &qp);CHKERRQ(ierr);
-    PTCHK(pt_op_set_eta_strided_h(c->op, &qp[0].eta, (int64_t)(sizeof(QPntVolCoefStokes) / sizeof(double))));
+  ierr = PetscObjectStateGet((PetscObject)gcoords, &st);CHKERRQ(ierr);
+  if (!b->have_coords || b->coords_vec != gcoords || b->coords_state != st) {
+    const PetscScalar *LA_gcoords;
+    ierr = VecGetArrayRead(gcoords, &LA_gcoords);CHKERRQ(ierr);
+    PTCHK(pt_op_set_coords_h(b->op, LA_gcoords));
+    ierr = VecRestoreArrayRead(gcoords, &LA_gcoords);CHKERRQ(ierr);
+    b->coords_vec = gcoords;
+    b->coords_state = st;
+    b->have_coords = PETSC_TRUE;
   }
-  c->have_data = PETSC_TRUE;
+  if (need_eta) {
+    int i, hit = -1;
+    for (i = 0; i < b->n_seen; i++)
+      if (b->eta_seen[i].key == key) hit = i;
+    if (!b->have_eta || hit < 0 || b->eta_seen[hit].state != key_state) {
+      QPntVolCoefStokes *qp;
+      ierr = VolumeQuadratureGetAllCellData_Stokes(volQ, &qp);CHKERRQ(ierr);
+      PTCHK(pt_op_set_eta_strided_h(b->op, &qp[0].eta, (int64_t)(sizeof(QPntVolCoefStokes) / sizeof(double))));
+      b->have_eta = PETSC_TRUE;
+      if (hit < 0) {
+        hit = b->n_seen < B200_ETA_KEYS ? b->n_seen++ : (b->next_slot++ % B200_ETA_KEYS);
+        b->eta_seen[hit].key = key;
+      }
+      b->eta_seen[hit].state = key_state;
+    }
+  }
+  PetscFunctionReturn(0);
+}
+
+/* The op of the velocity DM, for callers that want to hand it to the device
+ * solver (pt_solver_create) or read its counters. */
+PetscErrorCode MFA11B200GetOp(DM dau, pt_op **op)
+{
+  PetscErrorCode ierr;
+  B200Op *b;
+
+  PetscFunctionBeginUser;
+  ierr = B200_Shared(dau, &b, NULL);CHKERRQ(ierr);
+  *op = b->op;
   PetscFunctionReturn(0);
 }
 
@@ -110,7 +201,8 @@ PetscErrorCode MFA11SetUp_B200(MatA11MF mf)
 
   PetscFunctionBeginUser;
   if (mf->ctx) PetscFunctionReturn(0);
-  ierr = B200_Create(mf->daUVW, &c);CHKERRQ(ierr);
+  ierr = PetscCalloc1(1, &c);CHKERRQ(ierr);
+  ierr = B200_Shared(mf->daUVW, &c->b, &c->cont);CHKERRQ(ierr);
   mf->ctx = c;
   PetscFunctionReturn(0);
 }
@@ -122,12 +214,9 @@ PetscErrorCode MFStokesWrapper_A11_B200(MatA11MF mf, Quadrature volQ, DM dau, Pe
 
   PetscFunctionBeginUser;
   if (!c) SETERRQ(PETSC_COMM_SELF, PETSC_ERR_USER, "b200 MF-SpMV implementation should have a valid context");
-  if (!c->have_data || c->state != mf->state) {
-    ierr = B200_Upload(c, volQ, dau, PETSC_TRUE);CHKERRQ(ierr);
-    c->state = mf->state;
-  }
+  ierr = B200_Sync(c->b, dau, volQ, mf, mf->state, PETSC_TRUE);CHKERRQ(ierr);
   /* Yu was zeroed by the caller (stokes_operators.c:1195-1196): overwrite == add */
-  PTCHK(pt_a11_apply_h(c->op, ufield, Yu));
+  PTCHK(pt_a11_apply_h(c->b->op, ufield, Yu));
   PetscFunctionReturn(0);
 }
 
@@ -138,7 +227,7 @@ PetscErrorCode MFA11Destroy_B200(MatA11MF mf)
 
   PetscFunctionBeginUser;
   if (!c) SETERRQ(PETSC_COMM_SELF, PETSC_ERR_USER, "b200 MF-SpMV implementation should have a valid context");
-  PTCHK(pt_op_destroy(c->op));
+  ierr = PetscContainerDestroy(&c->cont);CHKERRQ(ierr);
   ierr = PetscFree(c);CHKERRQ(ierr);
   mf->ctx = NULL;
   PetscFunctionReturn(0);
@@ -157,89 +246,39 @@ PetscErrorCode MatA11MFRegister_B200(PetscFunctionList *matmult, PetscFunctionLi
   PetscFunctionReturn(0);
 }
 
-/* ---- diag / B / B^T: one op cached on the velocity DM ---------------------- */
+/* ---- diag / B / B^T / the whole operator ------------------------------------ */
 
-static PetscErrorCode B200_ContainerDestroy(void *ctx)
-{
-  MFA11B200 *c = (MFA11B200 *)ctx;
-  if (c) {
-    pt_op_destroy(c->op);
-    PetscFree(c);
-  }
-  return 0;
-}
-
-static PetscErrorCode B200_GetCached(DM dau, Quadrature volQ, PetscBool need_eta, MFA11B200 **out)
+/* Replaces MFStokesWrapper_diagA11 (src/stokes_operators_mf.c:71-135) inside
+ * MatGetDiagonal_MFStokes_A11, which passes its MatA11MF with mf->state set
+ * from the Mat (as MatMult_MFStokes_A11 does, stokes_operators.c:1176-1177). */
+PetscErrorCode MFStokesWrapper_diagA11_B200(MatA11MF mf, Quadrature volQ, DM dau, PetscScalar Yu[])
 {
   PetscErrorCode ierr;
-  PetscContainer cont = NULL;
-  MFA11B200 *c;
-  PetscObjectState st;
-
-  PetscFunctionBegin;
-  ierr = PetscObjectQuery((PetscObject)dau, "pt_b200_op", (PetscObject *)&cont);CHKERRQ(ierr);
-  if (!cont) {
-    ierr = B200_Create(dau, &c);CHKERRQ(ierr);
-    ierr = PetscContainerCreate(PetscObjectComm((PetscObject)dau), &cont);CHKERRQ(ierr);
-    ierr = PetscContainerSetPointer(cont, c);CHKERRQ(ierr);
-    ierr = PetscContainerSetUserDestroy(cont, B200_ContainerDestroy);CHKERRQ(ierr);
-    ierr = PetscObjectCompose((PetscObject)dau, "pt_b200_op", (PetscObject)cont);CHKERRQ(ierr);
-    ierr = PetscContainerDestroy(&cont);CHKERRQ(ierr);
-  } else {
-    ierr = PetscContainerGetPointer(cont, (void **)&c);CHKERRQ(ierr);
-  }
-  /* the coordinate Vec's state tracks mesh motion; re-upload when it moves */
-  {
-    Vec gcoords;
-    ierr = DMGetCoordinatesLocal(dau, &gcoords);CHKERRQ(ierr);
-    ierr = PetscObjectStateGet((PetscObject)gcoords, &st);CHKERRQ(ierr);
-  }
-  if (!c->have_data || c->state != st || need_eta) {
-    ierr = B200_Upload(c, volQ, dau, need_eta);CHKERRQ(ierr);
-    c->state = st;
-  }
-  *out = c;
-  PetscFunctionReturn(0);
-}
-
-/* Replaces MFStokesWrapper_diagA11 (src/stokes_operators_mf.c:71-135). */
-PetscErrorCode MFStokesWrapper_diagA11_B200(Quadrature volQ, DM dau, PetscScalar Yu[])
-{
-  PetscErrorCode ierr;
-  MFA11B200 *c;
+  B200Op *b;
 
   PetscFunctionBeginUser;
-  ierr = B200_GetCached(dau, volQ, PETSC_TRUE, &c);CHKERRQ(ierr);
-  PTCHK(pt_a11_diag_h(c->op, Yu));
+  if (mf->ctx) b = ((MFA11B200 *)mf->ctx)->b;
+  else {
+    ierr = B200_Shared(dau, &b, NULL);CHKERRQ(ierr);
+  }
+  ierr = B200_Sync(b, dau, volQ, mf, mf->state, PETSC_TRUE);CHKERRQ(ierr);
+  PTCHK(pt_a11_diag_h(b->op, Yu));
   PetscFunctionReturn(0);
 }
 
 /* Replaces MFStokesWrapper_A12_AVX / MFStokesWrapper_A12 (stokes_operators_avx.c:682,
- * stokes_operators_mf.c:792).  Pressure is element-local (4 dofs per element). */
+ * stokes_operators_mf.c:792).  Pressure is element-local (4 dofs per element);
+ * B^T depends on the coordinates only. */
 PetscErrorCode MFStokesWrapper_A12_B200(Quadrature volQ, DM dau, DM dap, PetscScalar Xp[], PetscScalar Yu[])
 {
   PetscErrorCode ierr;
-  MFA11B200 *c;
+  B200Op *b;
 
   PetscFunctionBeginUser;
   (void)dap;
-  ierr = B200_GetCached(dau, volQ, PETSC_FALSE, &c);CHKERRQ(ierr);
-  PTCHK(pt_a12_apply_h(c->op, Xp, Yu));
-  PetscFunctionReturn(0);
-}
-
-/* Replaces MFStokesWrapper_A_AVX / MFStokesWrapper_A (stokes_operators_avx.c:439,
- * stokes_operators_mf.c:711): Yu = A11 u + A12 p, Yp = A21 u in one call. */
-PetscErrorCode MFStokesWrapper_A_B200(Quadrature volQ, DM dau, PetscScalar ufield[], DM dap, PetscScalar pfield[],
-                                      PetscScalar Yu[], PetscScalar Yp[])
-{
-  PetscErrorCode ierr;
-  MFA11B200 *c;
-
-  PetscFunctionBeginUser;
-  (void)dap;
-  ierr = B200_GetCached(dau, volQ, PETSC_TRUE, &c);CHKERRQ(ierr);
-  PTCHK(pt_stokes_a_apply_h(c->op, ufield, pfield, Yu, Yp));
+  ierr = B200_Shared(dau, &b, NULL);CHKERRQ(ierr);
+  ierr = B200_Sync(b, dau, volQ, NULL, 0, PETSC_FALSE);CHKERRQ(ierr);
+  PTCHK(pt_a12_apply_h(b->op, Xp, Yu));
   PetscFunctionReturn(0);
 }
 
@@ -247,11 +286,32 @@ PetscErrorCode MFStokesWrapper_A_B200(Quadrature volQ, DM dau, PetscScalar ufiel
 PetscErrorCode MFStokesWrapper_A21_B200(Quadrature volQ, DM dau, DM dap, PetscScalar Xu[], PetscScalar Yp[])
 {
   PetscErrorCode ierr;
-  MFA11B200 *c;
+  B200Op *b;
 
   PetscFunctionBeginUser;
   (void)dap;
-  ierr = B200_GetCached(dau, volQ, PETSC_FALSE, &c);CHKERRQ(ierr);
-  PTCHK(pt_a21_apply_h(c->op, Xu, Yp));
+  ierr = B200_Shared(dau, &b, NULL);CHKERRQ(ierr);
+  ierr = B200_Sync(b, dau, volQ, NULL, 0, PETSC_FALSE);CHKERRQ(ierr);
+  PTCHK(pt_a21_apply_h(b->op, Xu, Yp));
+  PetscFunctionReturn(0);
+}
+
+/* Replaces MFStokesWrapper_A_AVX / MFStokesWrapper_A (stokes_operators_avx.c:439,
+ * stokes_operators_mf.c:711) inside MatMult_MFStokes_A: Yu = A11 u + A12 p,
+ * Yp = A21 u in one call.  A is the Stokes shell whose state versions the
+ * viscosity. */
+PetscErrorCode MFStokesWrapper_A_B200(Mat A, Quadrature volQ, DM dau, PetscScalar ufield[], DM dap,
+                                      PetscScalar pfield[], PetscScalar Yu[], PetscScalar Yp[])
+{
+  PetscErrorCode ierr;
+  B200Op *b;
+  PetscObjectState st;
+
+  PetscFunctionBeginUser;
+  (void)dap;
+  ierr = PetscObjectStateGet((PetscObject)A, &st);CHKERRQ(ierr);
+  ierr = B200_Shared(dau, &b, NULL);CHKERRQ(ierr);
+  ierr = B200_Sync(b, dau, volQ, A, st, PETSC_TRUE);CHKERRQ(ierr);
+  PTCHK(pt_stokes_a_apply_h(b->op, ufield, pfield, Yu, Yp));
   PetscFunctionReturn(0);
 }

@@ -22,7 +22,12 @@ def pytest_configure(config):
 def golden_names():
     """Operator fixtures (inputs and the reference's A11/diag/B/B^T/A outputs)."""
     return sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN_DIR, "*.npz"))
-                  if not os.path.basename(p).startswith("markers_"))
+                  if not os.path.basename(p).startswith(("markers_", "residual_")))
+
+
+def residual_golden_names():
+    """Momentum residual fixtures (FormFunctionLocal_U inputs and output)."""
+    return sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN_DIR, "residual_*.npz")))
 
 
 def marker_golden_names():

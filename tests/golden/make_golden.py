@@ -5,7 +5,7 @@ src/stokes_operators_{tensor,avx,mf}.c and src/element_utils_q{1,2}.c compiled
 unmodified (oracle/Makefile, Route A).  Inputs are seeded synthetic box meshes
 (ptatin-gene_b200/pt_b200/mesh.py).  Re-run after changing either:
 
-    python tests/golden/make_golden.py          (markers fixtures; operator fixtures if absent)
+    python tests/golden/make_golden.py          (markers and residual fixtures; operator fixtures if absent)
     python tests/golden/make_golden.py --all    (all fixtures)
 
 Each fixture stores the inputs and the reference outputs of
@@ -16,6 +16,13 @@ Each fixture stores the inputs and the reference outputs of
   the whole Stokes operator (Yu = A11 u + A12 p, Yp = A21 u) via "avx" and "ref"
   (MFStokesWrapper_A_AVX / MFStokesWrapper_A),
 all as unassembled local sums on one rank (local == global numbering).
+
+The residual fixtures (residual_*) store the inputs and output of the
+reference's momentum residual FormFunctionLocal_U
+(src/stokes_form_function.c:99-243): u with arbitrary values on Dirichlet dofs
+(the caller inserts boundary values, it does not zero them), p, the
+Gauss-point body force fu ([27 nel][3], QPntVolCoefStokes.Fu) and
+ru = A11 u + A12 p - body force, unassembled.
 The reference's OpenMP scatter ("omp critical") sums in thread order, so a
 re-run reproduces the A11 outputs only to ~1e-16 relative.
 """
@@ -43,6 +50,14 @@ CASES = {
 }
 
 
+RESIDUAL_CASES = {
+    # name: (workload, u seed, p seed, body-force seed)
+    "residual_c0_8x8x8": ("c0", 61, 62, 63),
+    "residual_box_3x2x4": ("box:3,2,4", 71, 72, 73),
+    "residual_box_1x1x3": ("box:1,1,3", 81, 82, 83),
+}
+
+
 MARKER_CASES = {
     # name: (workload, markers per element, seed)
     "markers_c0_8x8x8": ("c0", 6, 51),
@@ -58,6 +73,17 @@ def make_markers(name, workload, per_element, seed):
     eq, rq = oracle.RefCPU().marker_project(m.dims, wil, xi, eta, rho)
     np.savez_compressed(os.path.join(HERE, name + ".npz"), dims=np.array(m.dims, dtype=np.int32), wil=wil, xi=xi,
                         eta=eta, rho=rho, eta_qp=eq, rho_qp=rq)
+
+
+def make_residual(name, workload, useed, pseed, fseed):
+    """FormFunctionLocal_U of the reference (src/stokes_form_function.c:99-243)."""
+    m, eta, _ = M.problem(workload)
+    u = M.uniform_vec(m.nvel, useed)
+    p = M.uniform_vec(m.npres, pseed)
+    fu = M.uniform_vec(3 * 27 * m.nel, fseed)
+    ru = oracle.RefCPU().residual_u(m.dims, m.coords, eta, fu, u, p)
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), dims=np.array(m.dims, dtype=np.int32), coords=m.coords,
+                        eta=eta, fu=fu, u=u, p=p, ru=ru)
 
 
 def make(name, workload, useed, pseed, refvec):
@@ -91,4 +117,7 @@ if __name__ == "__main__":
             print("wrote", name)
     for name, args in MARKER_CASES.items():
         make_markers(name, *args)
+        print("wrote", name)
+    for name, args in RESIDUAL_CASES.items():
+        make_residual(name, *args)
         print("wrote", name)

@@ -3,7 +3,7 @@ reference's own operator sources (tests/golden/make_golden.py)."""
 import numpy as np
 import pytest
 
-from conftest import golden_names, load_golden, relerr
+from conftest import golden_names, load_golden, relerr, residual_golden_names
 
 # Bar for two FP64 implementations of the same operator with different
 # evaluation orders (the reference's own back-ends agree to ~1e-15).
@@ -86,3 +86,17 @@ def test_oracle_marker_projection_matches_reference(ora, name):
     assert relerr(rq, g["rho_qp"]) < 1e-13
     # values stay inside each element's node-value range (the clamp)
     assert np.all(eq >= g["eta"].min() * (1 - 1e-12)) and np.all(eq <= g["eta"].max() * (1 + 1e-12))
+
+
+@pytest.mark.parametrize("name", residual_golden_names())
+def test_oracle_residual_matches_reference(ora, name):
+    """The restated momentum residual against the reference's own
+    FormFunctionLocal_U (src/stokes_form_function.c:99-243), and the residual
+    as the sum of its parts: A11 u + A12 p minus the body-force load."""
+    g = load_golden(name)
+    dims = tuple(int(v) for v in g["dims"])
+    ru = ora.residual_u(dims, g["coords"], g["eta"], g["fu"], g["u"], g["p"])
+    assert relerr(ru, g["ru"]) < TOL
+    zero = ora.residual_u(dims, g["coords"], g["eta"], np.zeros_like(g["fu"]), g["u"], g["p"])
+    parts = ora.a11(dims, g["coords"], g["eta"], g["u"], "ref") + ora.a12(dims, g["coords"], g["p"], "ref")
+    assert relerr(zero, parts) < TOL
