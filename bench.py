@@ -380,6 +380,8 @@ def run_ours(args):
             dt = timed(fn, max(2, args.steps // 2)) / max(2, args.steps // 2)
             return n / dt / 1e9, dt * 1e3
         extra["a11_fp32_gdofs"], extra["a11_fp32_ms"] = rate(lambda: op.MatMult_MFStokes_A11(x32, y32), m.nvel)
+        # the SpMVOp-level apply (no Dirichlet columns or rows)
+        extra["a11_spmvop_gdofs"], extra["a11_spmvop_ms"] = rate(lambda: op.MFStokesWrapper_A11(x, y), m.nvel)
         extra["diag_gdofs"], extra["diag_ms"] = rate(lambda: op.MatGetDiagonal_MFStokes_A11(y), m.nvel)
         extra["a21_gdofs"], extra["a21_ms"] = rate(lambda: op.MatMult_MFStokes_A21(x, yp), m.nvel)
         extra["a12_gdofs"], extra["a12_ms"] = rate(lambda: op.MatMult_MFStokes_A12(p, y), m.nvel)

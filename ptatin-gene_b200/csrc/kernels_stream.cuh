@@ -156,14 +156,35 @@ __device__ __forceinline__ int64_t row_node0(const StreamGrid &g, int ex0, int e
   return g.b.off + 2 * (int64_t)ex0 + (2 * (int64_t)ej + r) * g.b.X + P * g.b.XY;
 }
 
+// Copies the words of the packed Dirichlet mask that cover the three rows of
+// node plane P into the slot's mask words (asynchronous 4-byte copies).
+template <int TX>
+__device__ __forceinline__ void stage_mask(uint32_t *mw, const StreamGrid &g, int ex0, int ej, int64_t P, int s,
+                                           const uint32_t *__restrict__ mbits)
+{
+  using L = TileLayout<TX>;
+  const int nd = 3 * min(L::NXN, 2 * (g.b.mx - ex0) + 1);
+#pragma unroll 1
+  for (int r = 0; r < 3; r++) {
+    const int64_t k0 = 3 * row_node0(g, ex0, ej, r, P);
+    const int64_t w0 = k0 >> 5;
+    const int nw = (int)(((k0 + nd - 1) >> 5) - w0 + 1);
+    if ((int)threadIdx.x < nw) {
+      const uint32_t dst = (uint32_t)__cvta_generic_to_shared(&mw[(s * 3 + r) * mask_row_words<TX>() + threadIdx.x]);
+      asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(dst), "l"(mbits + w0 + threadIdx.x) : "memory");
+    }
+  }
+}
+
 // Fetches node plane P (rows 0..2) of u into slot s with asynchronous 4- or
 // 8-byte copies straight into the component-planar tile (cp.async: no
-// registers, the copies run while the thread flushes y); with mbits, also the
-// words of the packed Dirichlet mask that cover each row.  The caller commits
-// and waits.
+// registers, the copies run while the thread flushes y).  MASKED: the
+// Dirichlet entries, whose bits the slot's staged mask words hold (visible to
+// every thread), are written as zeros instead -- the MatShell apply's column
+// rule.  The caller commits and waits.
 template <typename T, int TX, bool MASKED>
-__device__ __forceinline__ void fetch_plane(T *ut, uint32_t *mw, const StreamGrid &g, int ex0, int ej, int64_t P, int s,
-                                            const T *__restrict__ u, const uint32_t *__restrict__ mbits)
+__device__ __forceinline__ void fetch_plane(T *ut, const uint32_t *mw, const StreamGrid &g, int ex0, int ej, int64_t P,
+                                            int s, const T *__restrict__ u)
 {
   using L = TileLayout<TX>;
   const int nd = 3 * min(L::NXN, 2 * (g.b.mx - ex0) + 1);
@@ -171,53 +192,27 @@ __device__ __forceinline__ void fetch_plane(T *ut, uint32_t *mw, const StreamGri
   for (int r = 0; r < 3; r++) {
     const int64_t k0 = 3 * row_node0(g, ex0, ej, r, P);
     const T *src = u + k0;
+    const uint32_t *w = mw + (s * 3 + r) * mask_row_words<TX>();
+    const int b0 = (int)(k0 & 31);
     for (int d = threadIdx.x; d < nd; d += TX) {
       const int n = d / 3, c = d - 3 * n;
-      const uint32_t dst = (uint32_t)__cvta_generic_to_shared(&ut[L::at(c, s, r, n)]);
-      if (sizeof(T) == 8) asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(dst), "l"(src + d) : "memory");
-      else asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(dst), "l"(src + d) : "memory");
-    }
-    if (MASKED && mbits) {
-      const int64_t w0 = k0 >> 5;
-      const int nw = (int)(((k0 + nd - 1) >> 5) - w0 + 1);
-      if ((int)threadIdx.x < nw) {
-        const uint32_t dst = (uint32_t)__cvta_generic_to_shared(&mw[(s * 3 + r) * mask_row_words<TX>() + threadIdx.x]);
-        asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(dst), "l"(mbits + w0 + threadIdx.x) : "memory");
+      T *dst = &ut[L::at(c, s, r, n)];
+      if (MASKED) {
+        const int pos = b0 + d;
+        if ((w[pos >> 5] >> (pos & 31)) & 1u) {
+          *dst = T(0);
+          continue;
+        }
       }
+      const uint32_t sd = (uint32_t)__cvta_generic_to_shared(dst);
+      if (sizeof(T) == 8) asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(sd), "l"(src + d) : "memory");
+      else asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(sd), "l"(src + d) : "memory");
     }
   }
 }
 
 __device__ __forceinline__ void fetch_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void fetch_wait() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
-
-// Zeroes the Dirichlet entries of NP node planes P0, P0+1, .. (slots sl[])
-// after their fetch has landed and a barrier: the MatShell apply's column
-// rule.  One thread per staged mask word; it visits only the word's set bits,
-// so rows without Dirichlet dofs cost one shared load.
-template <typename T, int TX, int NP>
-__device__ __forceinline__ void mask_planes(T *ut, const uint32_t *mw, const StreamGrid &g, int ex0, int ej, int64_t P0,
-                                            const int *sl)
-{
-  using L = TileLayout<TX>;
-  constexpr int RW = mask_row_words<TX>();
-  const int nd = 3 * min(L::NXN, 2 * (g.b.mx - ex0) + 1);
-  for (int j = threadIdx.x; j < NP * 3 * RW; j += TX) {
-    const int p = j / (3 * RW), r = (j / RW) % 3, w = j % RW;
-    uint32_t bits = mw[(sl[p] * 3 + r) * RW + w];
-    if (!bits) continue;
-    const int b0 = (int)((3 * row_node0(g, ex0, ej, r, P0 + p)) & 31);
-    while (bits) {
-      const int b = __ffs(bits) - 1;
-      bits &= bits - 1;
-      const int d = 32 * w + b - b0;
-      if (d >= 0 && d < nd) {
-        const int n = d / 3, c = d - 3 * n;
-        ut[L::at(c, sl[p], r, n)] = T(0);
-      }
-    }
-  }
-}
 
 // L2 prefetch (TMA unit, no registers) of the u rows of node plane P, each
 // row segment rounded out to 16-byte boundaries inside the array of nu values.
@@ -249,16 +244,18 @@ __device__ __forceinline__ void zero_slot(T *yt, T *side, int s)
   }
 }
 
-// Flush node plane P (in slot s) to global y.  zshared: the plane is the
-// chunk's first/last plane and shared with a neighbouring chunk.  A node on a
+// Flush node plane P (in slot s) to global y, zeroing each y-tile (and side
+// buffer) entry as it is read, so the slot is ready for its next plane with
+// no further pass or barrier.  zshared: the plane is the chunk's first/last
+// plane and shared with a neighbouring chunk.  A node on a
 // tile boundary is stored by the first colour that touches it and added to
 // by the later ones; the colours are separate launches in a fixed order and
 // a launch touches each node from one CTA only, so the adds (red.global.add,
 // no read-back) happen in a fixed order: the sums are deterministic and equal
 // to a read-modify-write.  Dirichlet rows are set after the colour passes.
 template <typename T, int TX>
-__device__ __forceinline__ void flush_plane(const T *yt, const T *side, const StreamGrid &g, int tx, int ex0, int ej,
-                                            int64_t P, int s, bool zshared, T *__restrict__ y)
+__device__ __forceinline__ void flush_plane(T *yt, T *side, const StreamGrid &g, int tx, int ex0, int ej, int64_t P,
+                                            int s, bool zshared, T *__restrict__ y)
 {
   using L = TileLayout<TX>;
   const int nvalid = min(L::NXN, 2 * (g.b.mx - ex0) + 1);
@@ -272,7 +269,12 @@ __device__ __forceinline__ void flush_plane(const T *yt, const T *side, const St
     for (int d = threadIdx.x; d < nd; d += TX) {
       const int n = d / 3, c = d - 3 * n;
       T v = yt[L::at(c, s, r, n)];
-      if (L::NW > 1 && (n & 63) == 0 && n > 0 && n < 2 * TX) v += side[((n >> 6) - 1) * 27 + s * 9 + r * 3 + c];
+      yt[L::at(c, s, r, n)] = T(0);
+      if (L::NW > 1 && (n & 63) == 0 && n > 0 && n < 2 * TX) {
+        T *sb = &side[((n >> 6) - 1) * 27 + s * 9 + r * 3 + c];
+        v += *sb;
+        *sb = T(0);
+      }
       const int64_t k = 3 * node0 + d;
       const bool xb = (n == 0 && xlo) || (n == 2 * TX && xhi);
       const bool first = !((xb && g.px) || (yb && g.py) || (zshared && g.pz));
@@ -304,17 +306,31 @@ __device__ __forceinline__ void element_plane(const T *ut, T *yt, T *side, const
     q2::plane_fwd(Q, R, G[0][l], G[1][l], G[2][l]);
   }
 
-  // viscous action; K of the next point is loaded while this one computes
+  // viscous action.  FP64: K of the next two points is in flight while one
+  // computes (measured 2.18 -> 2.02 ms at 128^3, no spills); FP32, whose
+  // register budget is half, keeps one point of lookahead.
+  constexpr bool DEEP = sizeof(T) == 8;
   const T *kp = Ke + (int64_t)(9 * A) * 9 * MXP;
-  T Kn[9];
+  T Kn[9], Kn2[9];
 #pragma unroll
   for (int r = 0; r < 9; r++) Kn[r] = kp[(int64_t)r * MXP];
+  if (DEEP) {
+#pragma unroll
+    for (int r = 0; r < 9; r++) Kn2[r] = kp[(int64_t)(9 + r) * MXP];
+  }
 #pragma unroll
   for (int p = 0; p < 9; p++) {
     T Kq[9];
 #pragma unroll
     for (int r = 0; r < 9; r++) Kq[r] = Kn[r];
-    if (p < 8) {
+    if (DEEP) {
+#pragma unroll
+      for (int r = 0; r < 9; r++) Kn[r] = Kn2[r];
+      if (p < 7) {
+#pragma unroll
+        for (int r = 0; r < 9; r++) Kn2[r] = kp[(int64_t)(9 * (p + 2) + r) * MXP];
+      }
+    } else if (p < 8) {
 #pragma unroll
       for (int r = 0; r < 9; r++) Kn[r] = kp[(int64_t)(9 * (p + 1) + r) * MXP];
     }
@@ -376,21 +392,24 @@ __device__ __forceinline__ void stream_tile(const StreamGrid &g, int tx, int ej,
   // u holds at least the node planes up to the element box's last one
   const int64_t nu = 3 * g.b.XY * (int64_t)(g.b.off / g.b.XY + 2 * (int64_t)g.b.mz + 1);
 
-  // prologue: planes 2ek0 .. 2ek0+2 of u, zero y slots
+  // prologue: the Dirichlet words and then planes 2ek0 .. 2ek0+2 of u; zero y
+  if (MASKED) {
+    for (int k = 0; k < 3; k++) {
+      const int64_t P = 2 * (int64_t)ek0 + k;
+      stage_mask<TX>(mw, g, ex0, ej, P, (int)(P % 3), mbits);
+    }
+    fetch_commit();
+    fetch_wait();
+  }
+  for (int k = 0; k < 3; k++) zero_slot<T, TX>(yt, side, (int)((2 * (int64_t)ek0 + k) % 3));
+  __syncthreads();
   for (int k = 0; k < 3; k++) {
     const int64_t P = 2 * (int64_t)ek0 + k;
-    fetch_plane<T, TX, MASKED>(ut, mw, g, ex0, ej, P, (int)(P % 3), u, mbits);
+    fetch_plane<T, TX, MASKED>(ut, mw, g, ex0, ej, P, (int)(P % 3), u);
   }
   fetch_commit();
-  for (int k = 0; k < 3; k++) zero_slot<T, TX>(yt, side, (int)((2 * (int64_t)ek0 + k) % 3));
   fetch_wait();
   __syncthreads();
-  if (MASKED && mbits) {
-    const int sl0[3] = {(int)((2 * (int64_t)ek0) % 3), (int)((2 * (int64_t)ek0 + 1) % 3),
-                        (int)((2 * (int64_t)ek0 + 2) % 3)};
-    mask_planes<T, TX, 3>(ut, mw, g, ex0, ej, 2 * (int64_t)ek0, sl0);
-    __syncthreads();
-  }
 
   // the node column of a thread's i=2 nodes lives in the side buffer for
   // lane 31 of every warp but the last
@@ -404,10 +423,18 @@ __device__ __forceinline__ void stream_tile(const StreamGrid &g, int tx, int ej,
     const int s0 = (int)((2 * (int64_t)ek) % 3), s1 = (s0 + 1) % 3, s2 = (s0 + 2) % 3;
     const int sl[3] = {s0, s1, s2};
     const bool more = ek + 1 < ek1;
-    // the next layer's two new node planes go to L2 while this one computes
-    if (t == 32 && more) {
-      prefetch_u_plane<T, TX>(g, ex0, ej, 2 * (int64_t)ek + 3, u, nu);
-      prefetch_u_plane<T, TX>(g, ex0, ej, 2 * (int64_t)ek + 4, u, nu);
+    if (more) {
+      // the next layer's Dirichlet words land in the mask slots this layer no
+      // longer needs, and its two new node planes go to L2, while it computes
+      if (MASKED) {
+        stage_mask<TX>(mw, g, ex0, ej, 2 * (int64_t)ek + 3, s0, mbits);
+        stage_mask<TX>(mw, g, ex0, ej, 2 * (int64_t)ek + 4, s1, mbits);
+        fetch_commit();
+      }
+      if (t == 32) {
+        prefetch_u_plane<T, TX>(g, ex0, ej, 2 * (int64_t)ek + 3, u, nu);
+        prefetch_u_plane<T, TX>(g, ex0, ej, 2 * (int64_t)ek + 4, u, nu);
+      }
     }
 
     if (active) {
@@ -421,28 +448,23 @@ __device__ __forceinline__ void stream_tile(const StreamGrid &g, int tx, int ej,
       if (t == 0 && more) prefetch_k_plane(K + kidx(row + g.b.my, 0, 0, g.MXP, 0), kb);
       element_plane<T, TX, 2>(ut, yt, side, sl, t, warp, to_side, amask, K + krow, g.MXP);
     }
+    if (MASKED) fetch_wait();  // this thread's staged words
     __syncthreads();
 
     // u slots s0, s1 are free: node planes 2ek+3, 2ek+4 land there while
-    // planes 2ek and 2ek+1 (complete for this CTA) are flushed
+    // planes 2ek and 2ek+1 (complete for this CTA) are flushed and their y
+    // slots zeroed for the next layer
     if (more) {
-      fetch_plane<T, TX, MASKED>(ut, mw, g, ex0, ej, 2 * (int64_t)ek + 3, s0, u, mbits);
-      fetch_plane<T, TX, MASKED>(ut, mw, g, ex0, ej, 2 * (int64_t)ek + 4, s1, u, mbits);
+      fetch_plane<T, TX, MASKED>(ut, mw, g, ex0, ej, 2 * (int64_t)ek + 3, s0, u);
+      fetch_plane<T, TX, MASKED>(ut, mw, g, ex0, ej, 2 * (int64_t)ek + 4, s1, u);
       fetch_commit();
     }
     flush_plane<T, TX>(yt, side, g, tx, ex0, ej, 2 * (int64_t)ek, s0, ek == ek0 && zlo_shared, y);
     flush_plane<T, TX>(yt, side, g, tx, ex0, ej, 2 * (int64_t)ek + 1, s1, false, y);
     if (!more) flush_plane<T, TX>(yt, side, g, tx, ex0, ej, 2 * (int64_t)ek + 2, s2, zhi_shared, y);
     if (more) {
-      __syncthreads();  // the flush has read y slots s0, s1
-      zero_slot<T, TX>(yt, side, s0);
-      zero_slot<T, TX>(yt, side, s1);
       fetch_wait();
       __syncthreads();
-      if (MASKED && mbits) {
-        mask_planes<T, TX, 2>(ut, mw, g, ex0, ej, 2 * (int64_t)ek + 3, sl);
-        __syncthreads();
-      }
     }
   }
 }
