@@ -284,10 +284,33 @@ __device__ __forceinline__ void flush_plane(T *yt, T *side, const StreamGrid &g,
   }
 }
 
+// zeta contraction and its transpose for Gauss plane A given at run time:
+// rows A of B and D/h (q2_plane.cuh) from constant memory, so one copy of the
+// plane code serves all three planes (three unrolled copies measured 6-11%
+// slower: instruction fetch stalls).
+__constant__ double c_zB[3][3] = {{q2::B0, q2::B1, q2::B2}, {0.0, 1.0, 0.0}, {q2::B2, q2::B1, q2::B0}};
+__constant__ double c_zD[3][3] = {{q2::DZ00, q2::DZ01, q2::DZ02}, {-q2::GS, 0.0, q2::GS},
+                                  {q2::DZ20, q2::DZ21, q2::DZ22}};
+
+template <typename T>
+__device__ __forceinline__ void zeta_fwd_rt(int A, T n0, T n1, T n2, T &q, T &r)
+{
+  q = T(c_zB[A][0]) * n0 + (T(c_zB[A][1]) * n1 + T(c_zB[A][2]) * n2);
+  r = T(c_zD[A][0]) * n0 + (T(c_zD[A][1]) * n1 + T(c_zD[A][2]) * n2);
+}
+
+template <typename T>
+__device__ __forceinline__ void zeta_bwd_rt(int A, T q, T r, T &c0, T &c1, T &c2)
+{
+  c0 = T(c_zB[A][0]) * q + T(c_zD[A][0]) * r;
+  c1 = T(c_zB[A][1]) * q + T(c_zD[A][1]) * r;
+  c2 = T(c_zB[A][2]) * q + T(c_zD[A][2]) * r;
+}
+
 // One element (thread t of the tile), quadrature plane A: forward from the u
 // tile, viscous action with K, transpose accumulated into the y tile.
-template <typename T, int TX, int A>
-__device__ __forceinline__ void element_plane(const T *ut, T *yt, T *side, const int sl[3], int t, int warp,
+template <typename T, int TX>
+__device__ __forceinline__ void element_plane(int A, const T *ut, T *yt, T *side, const int sl[3], int t, int warp,
                                               bool to_side, unsigned amask, const T *__restrict__ Ke, int64_t MXP)
 {
   using L = TileLayout<TX>;
@@ -300,16 +323,15 @@ __device__ __forceinline__ void element_plane(const T *ut, T *yt, T *side, const
 #pragma unroll
       for (int i = 0; i < 3; i++) {
         const int n = 2 * t + i;
-        q2::zeta_fwd<T, A>(ut[L::at(l, sl[0], j, n)], ut[L::at(l, sl[1], j, n)], ut[L::at(l, sl[2], j, n)],
+        zeta_fwd_rt<T>(A, ut[L::at(l, sl[0], j, n)], ut[L::at(l, sl[1], j, n)], ut[L::at(l, sl[2], j, n)],
                            Q[3 * j + i], R[3 * j + i]);
       }
     q2::plane_fwd(Q, R, G[0][l], G[1][l], G[2][l]);
   }
 
-  // viscous action.  FP64: K of the next two points is in flight while one
-  // computes (measured 2.18 -> 2.02 ms at 128^3, no spills); FP32, whose
-  // register budget is half, keeps one point of lookahead.
-  constexpr bool DEEP = sizeof(T) == 8;
+  // viscous action: K of the next two points is in flight while one computes
+  // (measured at 128^3: FP64 2.18 -> 2.02 ms, FP32 1.20 -> 1.12 ms)
+  constexpr bool DEEP = true;
   const T *kp = Ke + (int64_t)(9 * A) * 9 * MXP;
   T Kn[9], Kn2[9];
 #pragma unroll
@@ -348,7 +370,7 @@ __device__ __forceinline__ void element_plane(const T *ut, T *yt, T *side, const
 #pragma unroll
       for (int j = 0; j < 3; j++) {
         T c0, c1, c2;
-        q2::zeta_bwd<T, A>(Qt[3 * j + i], Rt[3 * j + i], c0, c1, c2);
+        zeta_bwd_rt<T>(A, Qt[3 * j + i], Rt[3 * j + i], c0, c1, c2);
         if (i == 2 && to_side) {
           T *sb = side + warp * 27 + 3 * j + l;
           sb[sl[0] * 9] += c0;
@@ -441,12 +463,12 @@ __device__ __forceinline__ void stream_tile(const StreamGrid &g, int tx, int ej,
       // each quadrature plane's K is prefetched to L2 while the one before it computes
       const int64_t krow = kidx(row, 0, 0, g.MXP, ex);
       const uint32_t kb = (uint32_t)(sizeof(T) * 81 * g.MXP);
-      if (t == 0) prefetch_k_plane(K + kidx(row, 9, 0, g.MXP, 0), kb);
-      element_plane<T, TX, 0>(ut, yt, side, sl, t, warp, to_side, amask, K + krow, g.MXP);
-      if (t == 0) prefetch_k_plane(K + kidx(row, 18, 0, g.MXP, 0), kb);
-      element_plane<T, TX, 1>(ut, yt, side, sl, t, warp, to_side, amask, K + krow, g.MXP);
-      if (t == 0 && more) prefetch_k_plane(K + kidx(row + g.b.my, 0, 0, g.MXP, 0), kb);
-      element_plane<T, TX, 2>(ut, yt, side, sl, t, warp, to_side, amask, K + krow, g.MXP);
+#pragma unroll 1
+      for (int A = 0; A < 3; A++) {
+        if (t == 0 && (A < 2 || more))
+          prefetch_k_plane(A < 2 ? K + kidx(row, 9 * (A + 1), 0, g.MXP, 0) : K + kidx(row + g.b.my, 0, 0, g.MXP, 0), kb);
+        element_plane<T, TX>(A, ut, yt, side, sl, t, warp, to_side, amask, K + krow, g.MXP);
+      }
     }
     if (MASKED) fetch_wait();  // this thread's staged words
     __syncthreads();
