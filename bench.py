@@ -607,17 +607,34 @@ def run_batched(args):
     return 0
 
 
-def serve_requests(n, seed=0, sizes=(8, 48)):
+class RequestStream:
     """The served stream: cubic boxes m^3, m uniform over sizes; nodes
     perturbed +-0.05h; viscosity 1 with 8 seeded inclusions (radius 0.1), four
     at c^(1/2) and four at c^(-1/2), c log-uniform in [1e2, 1e6]; free-slip box
-    BCs; f uniform [-1, 1] on free dofs."""
-    from pt_b200 import mesh as M
-    rng = np.random.default_rng(seed)
-    out = []
-    for i in range(n):
-        m = int(rng.integers(sizes[0], sizes[1] + 1))
-        c = 10.0 ** rng.uniform(2.0, 6.0)
+    BCs; f uniform [-1, 1] on free dofs.  Request i is (mesh, eta, mask, f, c),
+    built on demand from its seeds (the size and contrast draws are made up
+    front, in order); start(ahead) builds requests in a background thread up to
+    `ahead` beyond the last one taken, so a long stream never holds more than a
+    window of requests in host memory."""
+
+    def __init__(self, n, seed=0, sizes=(8, 48)):
+        rng = np.random.default_rng(seed)
+        self.n, self.seed, self.draws = n, seed, []
+        for _ in range(n):
+            m = int(rng.integers(sizes[0], sizes[1] + 1))
+            self.draws.append((m, 10.0 ** rng.uniform(2.0, 6.0)))
+        self._ready, self._next, self._taken = {}, 0, 0
+        self._cv = threading.Condition()
+        self._thread = None
+        self.build_seconds = 0.0
+
+    def __len__(self):
+        return self.n
+
+    def make(self, i):
+        from pt_b200 import mesh as M
+        m, c = self.draws[i]
+        seed = self.seed
         mesh = M.make_mesh(m, m, m, perturb=0.05, seed=seed * 1000003 + i)
         r = np.random.default_rng(seed * 7919 + i + 1)
         centres = r.uniform(0.0, 1.0, size=(8, 3))
@@ -626,22 +643,63 @@ def serve_requests(n, seed=0, sizes=(8, 48)):
         mask = M.bc_mask_freeslip(m, m, m)
         f = M_uniform(mesh.nvel, seed * 31 + i)
         f[mask.astype(bool)] = 0.0
-        out.append((mesh, eta, mask, f, c))
-    return out
+        return mesh, eta, mask, f, c
+
+    def start(self, ahead=48):
+        def run():
+            while True:
+                with self._cv:
+                    while self._next < self.n and self._next >= self._taken + ahead:
+                        self._cv.wait()
+                    if self._next >= self.n:
+                        return
+                    i = self._next
+                    self._next += 1
+                t0 = time.perf_counter()
+                req = self.make(i)
+                with self._cv:
+                    self.build_seconds += time.perf_counter() - t0
+                    self._ready[i] = req
+                    self._cv.notify_all()
+        self._thread = threading.Thread(target=run, daemon=True)
+        self._thread.start()
+        return self
+
+    def take(self, i):
+        """Request i, in order; blocks until the producer has built it."""
+        if self._thread is None:
+            return self.make(i)
+        with self._cv:
+            while i not in self._ready:
+                self._cv.wait()
+            req = self._ready.pop(i)
+            self._taken = i + 1
+            self._cv.notify_all()
+        return req
 
 
-def serve_run(reqs, arrivals, iters, **opts):
-    """Serve reqs arriving at the given times (seconds on the server clock,
-    relative to the first arrival).  Returns (results by id, stats)."""
+def serve_requests(n, seed=0, sizes=(8, 48)):
+    """All n requests of the stream, built at once (short streams)."""
+    st = RequestStream(n, seed, sizes)
+    return [st.make(i) for i in range(n)]
+
+
+def serve_run(reqs, arrivals, iters, keep_x=None, **opts):
+    """Serve reqs (a list or a started RequestStream) arriving at the given
+    times (seconds on the server clock, relative to the first arrival).
+    Returns (results by id, stats); solutions are kept for the ids in keep_x
+    (all when None)."""
     from pt_b200.serve import Server
     res, max_active, max_bytes = {}, 0, 0
+    take = reqs.take if isinstance(reqs, RequestStream) else (lambda i: reqs[i])
+    n = len(reqs)
     with Server(**opts) as s:
         t0 = s.time()
         nxt = 0
-        while len(res) < len(reqs):
+        while len(res) < n:
             now = s.time() - t0
-            while nxt < len(reqs) and arrivals[nxt] <= now:
-                m, eta, mask, f, _ = reqs[nxt]
+            while nxt < n and arrivals[nxt] <= now:
+                m, eta, mask, f, _ = take(nxt)
                 s.submit(nxt, m.dims, m.coords, eta, mask, f)
                 nxt += 1
             act, queued = s.step(iters)
@@ -651,8 +709,10 @@ def serve_run(reqs, arrivals, iters, **opts):
                 d["t_done"] -= t0
                 d["t_submit"] -= t0
                 d["t_admit"] -= t0
+                if keep_x is not None and d["id"] not in keep_x:
+                    d.pop("x")
                 res[d["id"]] = d
-            if act == 0 and queued == 0 and nxt < len(reqs):
+            if act == 0 and queued == 0 and nxt < n:
                 time.sleep(max(0.0, min(0.01, arrivals[nxt] - (s.time() - t0))))
         st = s.stats()
     st.update(max_active=max_active, max_bytes_in_use=max_bytes)
@@ -671,7 +731,7 @@ def serve_leg(args, nreq, ncal, nserial):
     from pt_b200.solver import KSPSolveA11
     t_gen = time.time()
     cal = serve_requests(ncal, seed=1)
-    reqs = serve_requests(nreq, seed=0)
+    reqs = RequestStream(nreq, seed=0)
     t_gen = time.time() - t_gen
     # tile schedule (tile width, z-chunk depth) by the autotuner, on the
     # calibration requests' FP32 applies
@@ -695,20 +755,22 @@ def serve_leg(args, nreq, ncal, nserial):
     rng = np.random.default_rng(12345)
     arrivals = np.cumsum(rng.exponential(1.0 / rate, size=len(reqs)))
     arrivals -= arrivals[0]
-    res, st = serve_run(reqs, arrivals, args.serve_iters, **opts)
+    sample = list(range(0, len(reqs), max(1, len(reqs) // 8)))
+    reqs.start()
+    res, st = serve_run(reqs, arrivals, args.serve_iters, keep_x=set(sample), **opts)
     lat = np.array([res[i]["t_done"] - arrivals[i] for i in range(len(reqs))])
     wall = max(d["t_done"] for d in res.values())
     its = np.array([res[i]["its"] for i in range(len(reqs))])
     conv = all(res[i]["converged"] for i in range(len(reqs)))
     # true FP64 residual of a sample of served results
     relres = []
-    for i in range(0, len(reqs), max(1, len(reqs) // 8)):
-        m, eta, mask, f, _ = reqs[i]
+    for i in sample:
+        m, eta, mask, f, _ = reqs.make(i)
         relres.append(reference_residual(m, eta, mask, f, res[i]["x"]))
     # serial plain FP64 solves (one request at a time, set-up included)
     serial = []
     for i in np.linspace(0, len(reqs) - 1, min(nserial, len(reqs))).astype(int):
-        m, eta, mask, f, _ = reqs[i]
+        m, eta, mask, f, _ = reqs.make(int(i))
         torch.cuda.synchronize()
         t = time.time()
         with MatStokesMF(*m.dims) as op:
@@ -733,7 +795,11 @@ def serve_leg(args, nreq, ncal, nserial):
            "serial_mean_served_its_same_requests": float(np.mean([d["served_its"] for d in serial])),
            "speedup_solves_per_s": (len(reqs) / wall) / serial_rate, "server": st,
            "autotune": {"lz": lz, "tile_x": tile_x, "ms": {f"lz{a}_tx{b}": v for (a, b), v in table.items()}},
-           "host_generation_s": t_gen}
+           "host_generation_s": t_gen + reqs.build_seconds,
+           "latency_percentiles_s": {str(q): float(np.percentile(lat, q)) for q in (10, 25, 50, 75, 90, 95, 99, 99.9)},
+           "contrast_its": {f"1e{k}-1e{k + 1}": float(np.mean([res[i]["its"] for i in range(len(reqs))
+                                                              if 10 ** k <= reqs.draws[i][1] < 10 ** (k + 1)]))
+                            for k in (2, 3, 4, 5)}}
     return out
 
 
