@@ -206,6 +206,7 @@ typedef struct {
                            elements down is Galerkin, P^T A P element by element
                            (OP_TYPE_MFGALERKIN then OP_TYPE_GALERKIN,
                            src/ptatin_driver_linear_ts.c:64-380, 713-800) */
+  int32_t mg_fine_degree; /* PT_PC_MG: Chebyshev steps on the finest level (0 = cheby_degree) */
 } pt_solve_opts;
 
 typedef struct {

@@ -287,7 +287,7 @@ struct pt_mg_level {
 struct pt_mg {
   std::vector<pt_mg_level> lv;
   bool fp32;
-  int degree, coarse_degree;
+  int degree, coarse_degree, fine_degree;
   double emin, emax;
   int64_t fine_applies;  // A11 applies on level 0 inside V-cycles
   double coarse_work;    // coarse-level applies weighted by elements / fine elements
@@ -380,7 +380,8 @@ pt_status mg_vcycle(pt_mg &mg, int l)
     }
     return mg_cheby<T>(mg, L, b, x, true, mg.coarse_degree);
   }
-  if ((s = mg_cheby<T>(mg, L, b, x, true, mg.degree)) != PT_OK) return s;
+  const int degree = l == 0 ? mg.fine_degree : mg.degree;
+  if ((s = mg_cheby<T>(mg, L, b, x, true, degree)) != PT_OK) return s;
   // residual -> coarse rhs
   pt_mg_level &C = mg.lv[l + 1];
   if ((s = mg_matmult<T>(mg, L, x, (T *)L.az)) != PT_OK) return s;
@@ -406,7 +407,7 @@ pt_status mg_vcycle(pt_mg &mg, int l)
   PT_LAUNCHED(L.op);
   transfer_axis_kernel<T, 0, true, 1><<<vgrid(L.n), 256, 0, st>>>(dXf, dF, t1, x, L.op->d_mask);
   PT_LAUNCHED(L.op);
-  return mg_cheby<T>(mg, L, b, x, false, mg.degree);
+  return mg_cheby<T>(mg, L, b, x, false, degree);
 }
 
 }  // namespace

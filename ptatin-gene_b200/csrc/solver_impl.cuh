@@ -592,6 +592,7 @@ pt_status mg_build(pt_solver *s)
   s->mg = mg;  // freed by pt_solver_destroy, also after a failure here
   mg->fp32 = s->o.cheby_fp32 != 0;
   mg->degree = s->o.cheby_degree;
+  mg->fine_degree = s->o.mg_fine_degree > 0 ? s->o.mg_fine_degree : s->o.cheby_degree;
   mg->coarse_degree = s->o.mg_coarse_degree > 0 ? s->o.mg_coarse_degree : 24;
   mg->emin = s->o.cheby_emin;
   mg->emax = s->o.cheby_emax;
@@ -943,6 +944,7 @@ void pt_solve_opts_default(pt_solve_opts *o)
   o->mg_coarse_degree = 24;
   o->pc_graph = 1;
   o->mg_assembled = 2;
+  o->mg_fine_degree = 0;
 }
 
 pt_status pt_solver_create(pt_op *op, const pt_solve_opts *opts, pt_solver **out)
@@ -953,6 +955,8 @@ pt_status pt_solver_create(pt_op *op, const pt_solve_opts *opts, pt_solver **out
   if (opts->pc < PT_PC_NONE || opts->pc > PT_PC_MG) return fail(PT_ERR_BAD_ARG, "unknown pc %d", opts->pc);
   if (opts->restart < 1 || opts->restart > 256) return fail(PT_ERR_BAD_ARG, "restart must be in [1, 256]");
   if (opts->cheby_degree < 1 || opts->cheby_degree > 64) return fail(PT_ERR_BAD_ARG, "cheby_degree must be in [1, 64]");
+  if (opts->mg_fine_degree < 0 || opts->mg_fine_degree > 64)
+    return fail(PT_ERR_BAD_ARG, "mg_fine_degree must be in [0, 64]");
   if (!(opts->cheby_emin > 0.0) || !(opts->cheby_emax > opts->cheby_emin))
     return fail(PT_ERR_BAD_ARG, "need 0 < cheby_emin < cheby_emax");
   pt_status st = check_ready(op, true);
