@@ -55,9 +55,9 @@ WORKLOAD_TEXT = {
     "layered": "perturbed +-0.05h, layered eta + inclusions",
 }
 # DRAM bytes per element of one FP64 streaming apply (K 1.94 KB + u/y tiles),
-# measured with ncu on the 96^3 box: 2 colour launches averaged 0.730 GB for
-# 96^3/4 elements.
-TRAFFIC_PER_ELEMENT_F64 = 4 * 0.730e9 / 96 ** 3
+# measured with ncu on a 128x128x32 box (rows of 128 elements): 2 colour
+# launches averaged 0.327 GB read + 0.032 GB written for 128*128*32/4 elements.
+TRAFFIC_PER_ELEMENT_F64 = 4 * (0.327e9 + 0.032e9) / (128 * 128 * 32)
 UNIT = "GDoF/s"
 
 
@@ -450,8 +450,8 @@ def run_ours(args):
                        "a11_op": a11_op, "tiling": tiling, "l2": "inputs larger than L2 (no flush)"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": TRAFFIC_PER_ELEMENT_F64 * m.nel,
-                         "traffic_source": "ncu dram__bytes_read+write of the 4 colour launches of one 96^3 apply, "
-                                           "scaled by the element count",
+                         "traffic_source": "ncu dram__bytes_read+write per element of colour launches on a "
+                                           "128x128x32 box (rows of 128 elements), times the element count",
                          "peak_kind": peak_kind, "algorithmic_bytes_per_apply": bytes_alg},
             "cpu_baseline": cpu,
             "parity_relerr": parity["max"] if parity else None,
