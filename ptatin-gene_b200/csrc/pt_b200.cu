@@ -269,13 +269,16 @@ pt_status upload_diag_tables()
 // after an even one, or at the last chunk, so the node sums keep the order of
 // the whole-box launch (the even chunk of a boundary plane stores, the odd one
 // adds).
-template <typename T, int TX, bool MASKED>
-pt_status launch_stream_tx(pt_op *op, const T *K, const T *u, T *y, int zb = 0, int ze = -1)
+// KTX: one x-tile per row (MXP == TX), the K stride a compile-time constant
+// (FP64 only: it measured no faster in FP32).
+template <typename T, int TX, bool MASKED, bool KTX>
+pt_status launch_stream_tx_k(pt_op *op, const T *K, const T *u, T *y, int zb, int ze)
 {
   if (ze < 0) ze = op->nzc;
   if (MASKED && !op->d_mbits) return fail(PT_ERR_STATE, "masked apply without the packed Dirichlet bits");
+  if (KTX && op->MXP != TX) return fail(PT_ERR_STATE, "K row stride differs from the tile width");
   constexpr size_t smem = ptk::stream_smem_bytes<T, TX>();
-  pt_status as = kernel_attrs((const void *)ptk::a11_stream_kernel<T, TX, MASKED>, smem);
+  pt_status as = kernel_attrs((const void *)ptk::a11_stream_kernel<T, TX, MASKED, KTX>, smem);
   if (as != PT_OK) return as;
   ptk::StreamGrid g;
   g.b = op->box;
@@ -290,10 +293,19 @@ pt_status launch_stream_tx(pt_op *op, const T *K, const T *u, T *y, int zb = 0, 
         g.nzcc = g.zc0 < ze ? (ze - g.zc0 + 1) / 2 : 0;
         const int64_t n = (int64_t)g.nxc * g.nyc * g.nzcc;
         if (n == 0) continue;
-        ptk::a11_stream_kernel<T, TX, MASKED><<<(unsigned)n, TX, smem, op->stream>>>(g, K, u, MASKED ? op->d_mbits : nullptr, y);
+        ptk::a11_stream_kernel<T, TX, MASKED, KTX><<<(unsigned)n, TX, smem, op->stream>>>(g, K, u, MASKED ? op->d_mbits : nullptr, y);
         PT_LAUNCHED(op);
       }
   return PT_OK;
+}
+
+template <typename T, int TX, bool MASKED>
+pt_status launch_stream_tx(pt_op *op, const T *K, const T *u, T *y, int zb = 0, int ze = -1)
+{
+  if constexpr (sizeof(T) == 8) {
+    if (op->MXP == TX) return launch_stream_tx_k<T, TX, MASKED, true>(op, K, u, y, zb, ze);
+  }
+  return launch_stream_tx_k<T, TX, MASKED, false>(op, K, u, y, zb, ze);
 }
 
 template <typename T, bool MASKED>
