@@ -207,6 +207,10 @@ typedef struct {
                            (OP_TYPE_MFGALERKIN then OP_TYPE_GALERKIN,
                            src/ptatin_driver_linear_ts.c:64-380, 713-800) */
   int32_t mg_fine_degree; /* PT_PC_MG: Chebyshev steps on the finest level (0 = cheby_degree) */
+  int32_t mg_coarse_half; /* PT_PC_MG with cheby_fp32: Galerkin levels' element matrices kept in FP16, each
+                             element scaled by its largest entry, FP32 arithmetic (1, default: half the
+                             bytes of an FP32 copy); 0: FP32 copies.  Diagonal and lambda_max always come
+                             from the FP64 matrices. */
 } pt_solve_opts;
 
 typedef struct {

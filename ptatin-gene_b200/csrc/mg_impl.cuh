@@ -280,6 +280,8 @@ struct pt_mg_level {
   void *t1, *t2;                   // transfer temporaries (to / from the next coarser level)
   void *Ae, *ye;                   // element matrices and per-element outputs (small levels), else null
   double *Ae64;                    // Galerkin levels: FP64 element matrices P^T A P (Ae aliases or converts them)
+  __half *Ah;                      // Galerkin levels under FP32 smoothing: the matrices in FP16, scaled per
+  float *Ascale;                   // element by Ascale (mg_coarse_half), replacing an FP32 copy in Ae
   void *Ainv;                      // dense inverse (coarsest level, when small), else null
   int64_t nel;
 };
@@ -289,6 +291,7 @@ struct pt_mg {
   bool fp32;
   int degree, coarse_degree, fine_degree;
   double emin, emax;
+  bool coarse_half;      // FP32 smoothing: Galerkin levels' matrices stored in FP16 (scaled per element)
   int64_t fine_applies;  // A11 applies on level 0 inside V-cycles
   double coarse_work;    // coarse-level applies weighted by elements / fine elements
   bool assembled;  // element matrices on small levels, dense inverse on a small coarsest level
@@ -306,6 +309,18 @@ pt_status mg_matmult(pt_mg &mg, pt_mg_level &L, const T *x, T *y)
 {
   if (L.op == mg.lv[0].op) mg.fine_applies++;
   else mg.coarse_work += (double)L.op->nel / (double)mg.lv[0].op->nel;
+  if constexpr (std::is_same<T, float>::value) {
+    if (L.Ah) {
+      ebe_h_carveout<true>();
+      ptk::ebe_apply_h_kernel<true><<<(unsigned)L.nel, 96, 0, L.op->stream>>>(L.op->box, L.Ah, L.Ascale, x,
+                                                                               L.op->d_mask, (float *)L.ye);
+      PT_LAUNCHED(L.op);
+      ptk::ebe_gather_kernel<float, true><<<vgrid(L.n), 256, 0, L.op->stream>>>(L.op->box, (const float *)L.ye, x,
+                                                                                L.op->d_mask, y);
+      PT_LAUNCHED(L.op);
+      return PT_OK;
+    }
+  }
   if (L.Ae) {
     ebe_carveout<T, true>();
     ptk::ebe_apply_kernel<T, true><<<(unsigned)L.nel, 96, 0, L.op->stream>>>(L.op->box, (const T *)L.Ae, x,

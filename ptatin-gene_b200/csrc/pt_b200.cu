@@ -379,6 +379,12 @@ pt_status ebe_carveout()
   return kernel_attrs((const void *)ptk::ebe_apply_kernel<T, MASKED>, 0, true);
 }
 
+template <bool MASKED>
+pt_status ebe_h_carveout()
+{
+  return kernel_attrs((const void *)ptk::ebe_apply_h_kernel<MASKED>, 0, true);
+}
+
 template <typename T>
 pt_status launch_ebe(pt_op *op, const T *u, T *y, bool masked)
 {

@@ -367,7 +367,7 @@ void mg_free(pt_mg *mg)
   if (!mg) return;
   if (mg->gexec) cudaGraphExecDestroy(mg->gexec);
   for (pt_mg_level &L : mg->lv) {
-    void *p[] = {L.dinv64, L.dinv32, L.x, L.b, L.r, L.d, L.az, L.dl, L.t1, L.Ae, L.ye, L.Ainv};
+    void *p[] = {L.dinv64, L.dinv32, L.x, L.b, L.r, L.d, L.az, L.dl, L.t1, L.Ae, L.ye, L.Ainv, L.Ah, L.Ascale};
     for (void *q : p) cudaFree(q);
     if (L.Ae64 && (void *)L.Ae64 != L.Ae) cudaFree(L.Ae64);
     if (L.own && L.op) pt_op_destroy(L.op);
@@ -525,7 +525,12 @@ pt_status mg_level_setup(pt_solver *s, pt_mg &mg, pt_mg_level &L, const pt_op *n
     });
     if (st != PT_OK) return st;
     if (!next && L.n <= MG_DENSE_MAX_DOFS) return mg_dense_inverse(L, mg.fp32);
-    if (mg.fp32) {
+    if (mg.fp32 && mg.coarse_half) {
+      PT_CUDA(cudaMalloc(&L.Ah, sizeof(__half) * ptk::EBE_LD * L.nel));
+      PT_CUDA(cudaMalloc(&L.Ascale, sizeof(float) * L.nel));
+      ptk::ebe_to_half_kernel<<<(unsigned)L.nel, 128, 0, L.op->stream>>>(L.Ae64, L.Ah, L.Ascale);
+      PT_LAUNCHED(L.op);
+    } else if (mg.fp32) {
       PT_CUDA(cudaMalloc(&L.Ae, sizeof(float) * ptk::EBE_LD * L.nel));
       ptk::convert_kernel<float><<<vgrid(ptk::EBE_LD * L.nel), 256, 0, L.op->stream>>>(L.Ae64, (float *)L.Ae,
                                                                                      ptk::EBE_LD * L.nel);
@@ -596,6 +601,7 @@ pt_status mg_build(pt_solver *s)
   mg->coarse_degree = s->o.mg_coarse_degree > 0 ? s->o.mg_coarse_degree : 24;
   mg->emin = s->o.cheby_emin;
   mg->emax = s->o.cheby_emax;
+  mg->coarse_half = s->o.mg_coarse_half != 0;
   mg->use_graph = s->o.pc_graph != 0;
   mg->assembled = s->o.mg_assembled != 0;
   const int maxl = s->o.mg_levels > 0 ? s->o.mg_levels : 32;
@@ -945,6 +951,7 @@ void pt_solve_opts_default(pt_solve_opts *o)
   o->pc_graph = 1;
   o->mg_assembled = 2;
   o->mg_fine_degree = 0;
+  o->mg_coarse_half = 1;
 }
 
 pt_status pt_solver_create(pt_op *op, const pt_solve_opts *opts, pt_solver **out)
@@ -957,6 +964,8 @@ pt_status pt_solver_create(pt_op *op, const pt_solve_opts *opts, pt_solver **out
   if (opts->cheby_degree < 1 || opts->cheby_degree > 64) return fail(PT_ERR_BAD_ARG, "cheby_degree must be in [1, 64]");
   if (opts->mg_fine_degree < 0 || opts->mg_fine_degree > 64)
     return fail(PT_ERR_BAD_ARG, "mg_fine_degree must be in [0, 64]");
+  if (opts->mg_coarse_half != 0 && opts->mg_coarse_half != 1)
+    return fail(PT_ERR_BAD_ARG, "mg_coarse_half must be 0 or 1");
   if (!(opts->cheby_emin > 0.0) || !(opts->cheby_emax > opts->cheby_emin))
     return fail(PT_ERR_BAD_ARG, "need 0 < cheby_emin < cheby_emax");
   pt_status st = check_ready(op, true);

@@ -32,7 +32,8 @@ class SolveOpts(ctypes.Structure):
                 ("cheby_degree", ctypes.c_int32), ("cheby_fp32", ctypes.c_int32),
                 ("cheby_emin", ctypes.c_double), ("cheby_emax", ctypes.c_double), ("eig_its", ctypes.c_int32),
                 ("mg_levels", ctypes.c_int32), ("mg_coarse_degree", ctypes.c_int32), ("pc_graph", ctypes.c_int32),
-                ("mg_assembled", ctypes.c_int32), ("mg_fine_degree", ctypes.c_int32)]
+                ("mg_assembled", ctypes.c_int32), ("mg_fine_degree", ctypes.c_int32),
+                ("mg_coarse_half", ctypes.c_int32)]
 
 
 class SolveStats(ctypes.Structure):

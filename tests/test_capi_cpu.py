@@ -92,5 +92,5 @@ def test_solver_defaults_without_device():
     assert o.ksp == KSP["fgmres"] and o.restart == 30 and o.rtol == 1e-8
     assert o.cheby_degree == 3 and o.cheby_fp32 == 1
     assert (o.cheby_emin, o.cheby_emax) == (0.2, 1.1)
-    assert o.mg_assembled == 2 and o.pc_graph == 1 and o.mg_fine_degree == 0
+    assert o.mg_assembled == 2 and o.pc_graph == 1 and o.mg_fine_degree == 0 and o.mg_coarse_half == 1
     assert PC["mg"] == 3

@@ -298,3 +298,36 @@ def test_mg_dense_coarsest_level_is_an_exact_solve(ora):
         st = k.solve(fd, x)
     assert st["converged"] and st["its"] <= 2, st
     assert relerr(x.cpu().numpy(), xref) < 1e-10
+
+
+def test_mg_fp16_coarse_matrices_keep_convergence(ora):
+    """FP32 smoothing with the Galerkin levels' element matrices in FP16
+    (scaled per element, mg_coarse_half=1, the default) against FP32 copies
+    (mg_coarse_half=0) on a 1e6-contrast layered box: both reach rtol on the
+    true residual of the reference's own A11, in about the same number of
+    iterations, and the solutions agree."""
+    import torch
+
+    from pt_b200.solver import KSPSolveA11
+    m, eta, mask, f, op, fd = setup("layered:16,16,16", seed=5)
+    xs, its = {}, {}
+    with op:
+        for half in (0, 1):
+            x = torch.zeros_like(fd)
+            with KSPSolveA11(op, pc="mg", ksp="fcg", cheby_fp32=1, mg_coarse_half=half, rtol=1e-9,
+                             max_it=4000) as k:
+                st = k.solve(fd, x)
+            assert st["converged"] == 1, (half, st)
+            xs[half], its[half] = x.cpu().numpy(), st["its"]
+    assert its[1] <= 1.1 * its[0] + 2, its
+    assert true_relres(ora, m, eta, mask, f, xs[1]) < 2e-9
+    assert relerr(xs[1], xs[0]) < 1e-6
+
+
+def test_mg_coarse_half_option_is_checked():
+    from pt_b200 import PtError
+    from pt_b200.solver import KSPSolveA11
+    m, eta, mask, f, op, fd = setup("box:8,8,8", seed=2)
+    with op:
+        with pytest.raises(PtError, match="mg_coarse_half"):
+            KSPSolveA11(op, pc="mg", mg_coarse_half=2)
