@@ -411,6 +411,12 @@ __device__ __forceinline__ void stream_tile(const StreamGrid &g, int tx, int ej,
   T *side = yt + L::TILE;
   uint32_t *mw = reinterpret_cast<uint32_t *>(side + L::SIDE);
   const int ex0 = tx * TX;
+  // Programmatic dependent launch: once every CTA of this grid has started,
+  // a grid launched after it with programmatic stream serialization may
+  // begin on the SMs this grid frees (its prologue and first layer overlap
+  // this grid's last wave); that grid waits below before writing y.  Both
+  // instructions do nothing for an ordinary launch.
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
   const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
   const int ex = ex0 + t;
   const bool active = ex < g.b.mx;
@@ -486,6 +492,12 @@ __device__ __forceinline__ void stream_tile(const StreamGrid &g, int tx, int ej,
       fetch_plane<T, TX, MASKED>(ut, mw, g, ex0, ej, 2 * (int64_t)ek + 4, s1, u);
       fetch_commit();
     }
+    // y is written from here on: the previous grid in the stream (an earlier
+    // colour of this apply, when launched programmatically) must be complete
+    // and its stores visible.  u, K and the mask bits are read before this
+    // point, so a programmatic launch is only made where the previous grid
+    // does not write them (the colours after the first of one apply).
+    if (ek == ek0) asm volatile("griddepcontrol.wait;" ::: "memory");
     flush_plane<T, TX>(yt, side, g, tx, ex0, ej, 2 * (int64_t)ek, s0, ek == ek0 && zlo_shared, y);
     flush_plane<T, TX>(yt, side, g, tx, ex0, ej, 2 * (int64_t)ek + 1, s1, false, y);
     if (!more) flush_plane<T, TX>(yt, side, g, tx, ex0, ej, 2 * (int64_t)ek + 2, s2, zhi_shared, y);
