@@ -31,16 +31,30 @@ struct pt_batch {
 
 namespace {
 
+// programmatic: a class after the first of one apply may start on the SMs
+// the previous class frees; the tile waits in-kernel before writing y (the
+// classes of one apply read the same u, K and mask bits)
 template <typename T, int TX, bool MASKED>
-pt_status batch_launch_cls(const pt_batch *b, const pt_batch::Cls &c, const T *const *u, T *const *y, cudaStream_t st)
+pt_status batch_launch_cls(const pt_batch *b, const pt_batch::Cls &c, const T *const *u, T *const *y, cudaStream_t st,
+                           bool programmatic)
 {
   constexpr size_t smem = ptk::stream_smem_bytes<T, TX>();
   pt_status as = kernel_attrs((const void *)ptk::a11_stream_batch_kernel<T, TX, MASKED>, smem);
   if (as != PT_OK) return as;
   const ptk::BatchProb *probs = std::is_same<T, double>::value ? b->d_probs64 : b->d_probs32;
-  ptk::a11_stream_batch_kernel<T, TX, MASKED>
-      <<<(unsigned)c.count, TX, smem, st>>>(probs, b->d_items + c.off, c.px, c.py, c.pz, u, y);
-  cudaError_t e = cudaGetLastError();
+  cudaLaunchAttribute pdl[1];
+  pdl[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  pdl[0].val.programmaticStreamSerializationAllowed = 1;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)c.count);
+  cfg.blockDim = dim3(TX);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cfg.attrs = programmatic ? pdl : nullptr;
+  cfg.numAttrs = programmatic ? 1 : 0;
+  const int4 *items = b->d_items + c.off;
+  const cudaError_t e = cudaLaunchKernelEx(&cfg, ptk::a11_stream_batch_kernel<T, TX, MASKED>, probs, items, c.px, c.py,
+                                           c.pz, u, y);
   if (e != cudaSuccess) return fail(PT_ERR_CUDA, "batched kernel launch: %s", cudaGetErrorString(e));
   return PT_OK;
 }
@@ -66,12 +80,14 @@ pt_status batch_apply(pt_batch *b, const T *const *u, T *const *y, void *stream)
 {
   if (!b || !u || !y) return fail(PT_ERR_BAD_ARG, "NULL argument");
   const cudaStream_t st = (cudaStream_t)stream;
+  bool first = true;
   for (const pt_batch::Cls &c : b->classes) {
     pt_status s;
-    if (c.TX == 32) s = batch_launch_cls<T, 32, MASKED>(b, c, u, y, st);
-    else if (c.TX == 64) s = batch_launch_cls<T, 64, MASKED>(b, c, u, y, st);
-    else s = batch_launch_cls<T, 128, MASKED>(b, c, u, y, st);
+    if (c.TX == 32) s = batch_launch_cls<T, 32, MASKED>(b, c, u, y, st, !first);
+    else if (c.TX == 64) s = batch_launch_cls<T, 64, MASKED>(b, c, u, y, st, !first);
+    else s = batch_launch_cls<T, 128, MASKED>(b, c, u, y, st, !first);
     if (s != PT_OK) return s;
+    first = false;
   }
   if (MASKED) {
     const ptk::BatchProb *probs = std::is_same<T, double>::value ? b->d_probs64 : b->d_probs32;
