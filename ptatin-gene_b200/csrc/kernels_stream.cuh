@@ -184,7 +184,7 @@ __device__ __forceinline__ void stage_mask(uint32_t *mw, const StreamGrid &g, in
 // rule.  The caller commits and waits.
 template <typename T, int TX, bool MASKED>
 __device__ __forceinline__ void fetch_plane(T *ut, const uint32_t *mw, const StreamGrid &g, int ex0, int ej, int64_t P,
-                                            int s, const T *__restrict__ u)
+                                            int s, const T *__restrict__ u, bool mk)
 {
   using L = TileLayout<TX>;
   const int nd = 3 * min(L::NXN, 2 * (g.b.mx - ex0) + 1);
@@ -197,7 +197,7 @@ __device__ __forceinline__ void fetch_plane(T *ut, const uint32_t *mw, const Str
     for (int d = threadIdx.x; d < nd; d += TX) {
       const int n = d / 3, c = d - 3 * n;
       T *dst = &ut[L::at(c, s, r, n)];
-      if (MASKED) {
+      if (MASKED && mk) {
         const int pos = b0 + d;
         if ((w[pos >> 5] >> (pos & 31)) & 1u) {
           *dst = T(0);
@@ -398,7 +398,7 @@ __device__ __forceinline__ void element_plane(int A, const T *ut, T *yt, T *side
 // One tile (x-tile tx, row ej, z-chunk zc) of one problem; the whole CTA.
 // MASKED (and mbits non-null): Dirichlet columns of u zeroed from the packed
 // mask mbits.  KTX: g.MXP == TX (one x-tile per row).
-template <typename T, int TX, bool MASKED, bool KTX = false>
+template <typename T, int TX, bool MASKED, bool KTX = false, bool NULLABLE = false>
 __device__ __forceinline__ void stream_tile(const StreamGrid &g, int tx, int ej, int zc, const T *__restrict__ K,
                                             const T *__restrict__ u, const uint32_t *__restrict__ mbits,
                                             T *__restrict__ y)
@@ -425,8 +425,13 @@ __device__ __forceinline__ void stream_tile(const StreamGrid &g, int tx, int ej,
   // u holds at least the node planes up to the element box's last one
   const int64_t nu = 3 * g.b.XY * (int64_t)(g.b.off / g.b.XY + 2 * (int64_t)g.b.mz + 1);
 
+  // masked apply of a problem that has a mask (a batched apply mixes boxes
+  // with and without one, NULLABLE: those get the plain apply and read no
+  // mask; a single-op masked launch always has the packed bits)
+  const bool mk = MASKED && (!NULLABLE || mbits != nullptr);
+
   // prologue: the Dirichlet words and then planes 2ek0 .. 2ek0+2 of u; zero y
-  if (MASKED) {
+  if (mk) {
     for (int k = 0; k < 3; k++) {
       const int64_t P = 2 * (int64_t)ek0 + k;
       stage_mask<TX>(mw, g, ex0, ej, P, (int)(P % 3), mbits);
@@ -438,7 +443,7 @@ __device__ __forceinline__ void stream_tile(const StreamGrid &g, int tx, int ej,
   __syncthreads();
   for (int k = 0; k < 3; k++) {
     const int64_t P = 2 * (int64_t)ek0 + k;
-    fetch_plane<T, TX, MASKED>(ut, mw, g, ex0, ej, P, (int)(P % 3), u);
+    fetch_plane<T, TX, MASKED>(ut, mw, g, ex0, ej, P, (int)(P % 3), u, mk);
   }
   fetch_commit();
   fetch_wait();
@@ -459,7 +464,7 @@ __device__ __forceinline__ void stream_tile(const StreamGrid &g, int tx, int ej,
     if (more) {
       // the next layer's Dirichlet words land in the mask slots this layer no
       // longer needs, and its two new node planes go to L2, while it computes
-      if (MASKED) {
+      if (mk) {
         stage_mask<TX>(mw, g, ex0, ej, 2 * (int64_t)ek + 3, s0, mbits);
         stage_mask<TX>(mw, g, ex0, ej, 2 * (int64_t)ek + 4, s1, mbits);
         fetch_commit();
@@ -481,15 +486,15 @@ __device__ __forceinline__ void stream_tile(const StreamGrid &g, int tx, int ej,
         element_plane<T, TX, KTX>(A, ut, yt, side, sl, t, warp, to_side, amask, K + krow, MXP);
       }
     }
-    if (MASKED) fetch_wait();  // this thread's staged words
+    if (mk) fetch_wait();  // this thread's staged words
     __syncthreads();
 
     // u slots s0, s1 are free: node planes 2ek+3, 2ek+4 land there while
     // planes 2ek and 2ek+1 (complete for this CTA) are flushed and their y
     // slots zeroed for the next layer
     if (more) {
-      fetch_plane<T, TX, MASKED>(ut, mw, g, ex0, ej, 2 * (int64_t)ek + 3, s0, u);
-      fetch_plane<T, TX, MASKED>(ut, mw, g, ex0, ej, 2 * (int64_t)ek + 4, s1, u);
+      fetch_plane<T, TX, MASKED>(ut, mw, g, ex0, ej, 2 * (int64_t)ek + 3, s0, u, mk);
+      fetch_plane<T, TX, MASKED>(ut, mw, g, ex0, ej, 2 * (int64_t)ek + 4, s1, u, mk);
       fetch_commit();
     }
     // y is written from here on: the previous grid in the stream (an earlier
@@ -561,7 +566,7 @@ __global__ void __launch_bounds__(TX, stream_min_blocks<T, TX>()) a11_stream_bat
   g.px = px; g.py = py; g.pz = pz;
   g.nxc = g.nyc = g.nzcc = 0;
   g.zc0 = pz;
-  stream_tile<T, TX, MASKED>(g, it.y, it.z, it.w, reinterpret_cast<const T *>(p.K), uptr[it.x],
+  stream_tile<T, TX, MASKED, false, true>(g, it.y, it.z, it.w, reinterpret_cast<const T *>(p.K), uptr[it.x],
                              MASKED ? p.mbits : nullptr, yptr[it.x]);
 }
 

@@ -72,3 +72,36 @@ def test_batched_matches_oracle(problems, ora):
         eta = M.eta_per_element(m, contrast=10.0 ** (2 + 2 * (i % 3)), seed=i)
         ref = ora.matmult_a11(m.dims, m.coords, eta, M.bc_mask_freeslip(mx, my, mz), u.cpu().numpy())
         assert relerr(y.cpu().numpy(), ref) < 1e-12, (mx, my, mz)
+
+
+@pytest.mark.parametrize("fp32", [False, True])
+def test_masked_batch_mixes_boxes_with_and_without_a_mask(fp32):
+    """A MatShell-level (masked) batched apply over boxes of which some carry
+    no Dirichlet mask: those get the plain apply, the others the column and
+    row rules, each bitwise its own op's MatMult (the served form submits
+    requests with or without a mask into one masked batch)."""
+    import torch
+
+    from pt_b200 import MatStokesMF
+    from pt_b200.batch import BatchA11
+    ops, us = [], []
+    try:
+        for i, (mx, my, mz) in enumerate([(8, 8, 8), (12, 6, 9), (20, 4, 5)]):
+            m = M.make_mesh(mx, my, mz, perturb=0.05, seed=40 + i)
+            eta = M.eta_per_element(m, contrast=1e4, seed=40 + i)
+            op = MatStokesMF(mx, my, mz, a11_op="b200_stream")
+            op.SetUp(m.coords, eta, M.bc_mask_freeslip(mx, my, mz) if i != 1 else None)
+            ops.append(op)
+            u = torch.from_numpy(M.uniform_vec(m.nvel, 60 + i)).cuda()
+            us.append(u.float() if fp32 else u)
+        ys = [torch.full_like(u, float("nan")) for u in us]
+        with BatchA11(ops) as b:
+            b.apply(us, ys, masked=True)
+            torch.cuda.synchronize()
+        for op, u, y in zip(ops, us, ys):
+            ref = op.MatMult_MFStokes_A11(u)
+            torch.cuda.synchronize()
+            assert torch.equal(y, ref)
+    finally:
+        for op in ops:
+            op.Destroy()

@@ -110,3 +110,20 @@ def test_serving_matches_single_solver(ora):
         st = k.solve(torch.from_numpy(f).cuda(), x)
     assert st["converged"]
     assert relerr(d["x"], x.cpu().numpy()) < 1e-6
+
+
+def test_request_without_a_mask_shares_the_batch():
+    """A request submitted without a Dirichlet mask runs in the same masked
+    batch as the others (plain apply for it, no mask read): it finishes with
+    finite values, and a masked request beside it is bitwise what it is alone."""
+    from pt_b200.serve import Server
+    m, eta, mask, f = request("box:6,5,4", 7)
+    m2, eta2, _, f2 = request("box:5,4,4", 8)
+    with Server(cheby_fp32=1, rtol=1e-8, max_it=300) as s:
+        alone = run(s, {0: (m, eta, mask, f)}, {0: [0]})
+    with Server(cheby_fp32=1, rtol=1e-8, max_it=300) as s:
+        mixed = run(s, {0: (m, eta, mask, f), 1: (m2, eta2, None, f2)}, {0: [0, 1]})
+    assert sorted(mixed) == [0, 1]
+    assert alone[0]["converged"] == 1
+    assert np.array_equal(mixed[0]["x"], alone[0]["x"])
+    assert np.isfinite(mixed[1]["x"]).all()
