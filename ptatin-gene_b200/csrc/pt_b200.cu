@@ -22,6 +22,7 @@
 #include "pt_b200.h"
 #include "kernels_colour.cuh"
 #include "kernels_stream.cuh"
+#include "kernels_diag.cuh"
 #include "kernels_ebe.cuh"
 #include "kernels_markers.cuh"
 #include "kernels_bmat.cuh"
@@ -268,34 +269,24 @@ pt_status upload_diag_tables()
 
 // ---- streaming kernel: geometry set-up and launch -----------------------------
 
-// Launches the streaming kernel's colour passes over z-chunks [zb, ze)
-// (ze < 0: all).  A sub-range must start at chunk 0 or at an odd chunk and end
-// after an even one, or at the last chunk, so the node sums keep the order of
-// the whole-box launch (the even chunk of a boundary plane stores, the odd one
-// adds).
-// KTX: one x-tile per row (MXP == TX), the K stride a compile-time constant
-// (FP64 only: it measured no faster in FP32).
-template <typename T, int TX, bool MASKED, bool KTX>
-pt_status launch_stream_tx_k(pt_op *op, const T *K, const T *u, T *y, int zb, int ze)
+// Enumerates the colour classes of the streaming tiles over z-chunks [zb, ze)
+// in their fixed order and calls launch(cfg, g) for each non-empty class with
+// the grid and launch configuration filled in.  The first launch is ordinary
+// (the grid before it may write the kernel's inputs); the later ones are
+// programmatic: each may start on the SMs the previous colour frees and waits
+// inside before writing its output (measured at 128^3: 1.74 -> 1.63 ms with
+// every A11 colour programmatic, bitwise the same result).
+template <int TX, typename F>
+pt_status stream_colours(pt_op *op, size_t smem, int zb, int ze, F &&launch)
 {
   if (ze < 0) ze = op->nzc;
-  if (MASKED && !op->d_mbits) return fail(PT_ERR_STATE, "masked apply without the packed Dirichlet bits");
-  if (KTX && op->MXP != TX) return fail(PT_ERR_STATE, "K row stride differs from the tile width");
-  constexpr size_t smem = ptk::stream_smem_bytes<T, TX>();
-  pt_status as = kernel_attrs((const void *)ptk::a11_stream_kernel<T, TX, MASKED, KTX>, smem);
-  if (as != PT_OK) return as;
   ptk::StreamGrid g;
   g.b = op->box;
   g.TX = TX; g.ntx = op->ntx; g.LZ = op->LZ; g.nzc = op->nzc; g.MXP = op->MXP;
-  // the first colour is an ordinary launch (the grid before it may write u);
-  // the later ones are programmatic: each may start on the SMs the previous
-  // colour frees and waits inside before writing y (measured at 128^3: 1.74
-  // -> 1.63 ms with every colour programmatic, bitwise the same result)
-  cudaLaunchAttribute pdl[1];
+  cudaLaunchAttribute pdl[1] = {};
   pdl[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
   pdl[0].val.programmaticStreamSerializationAllowed = 1;
   bool first = true;
-  const uint32_t *mb = MASKED ? op->d_mbits : nullptr;
   for (int pz = 0; pz < 2; pz++)
     for (int py = 0; py < 2; py++)
       for (int px = 0; px < 2; px++) {
@@ -313,12 +304,35 @@ pt_status launch_stream_tx_k(pt_op *op, const T *K, const T *u, T *y, int zb, in
         cfg.stream = op->stream;
         cfg.attrs = first ? nullptr : pdl;
         cfg.numAttrs = first ? 0 : 1;
-        const cudaError_t e = cudaLaunchKernelEx(&cfg, ptk::a11_stream_kernel<T, TX, MASKED, KTX>, g, K, u, mb, y);
-        if (e != cudaSuccess) return fail(PT_ERR_CUDA, "streaming A11 launch: %s", cudaGetErrorString(e));
+        pt_status s = launch(cfg, g);
+        if (s != PT_OK) return s;
         PT_LAUNCHED(op);
         first = false;
       }
   return PT_OK;
+}
+
+// Launches the streaming kernel's colour passes over z-chunks [zb, ze)
+// (ze < 0: all).  A sub-range must start at chunk 0 or at an odd chunk and end
+// after an even one, or at the last chunk, so the node sums keep the order of
+// the whole-box launch (the even chunk of a boundary plane stores, the odd one
+// adds).
+// KTX: one x-tile per row (MXP == TX), the K stride a compile-time constant
+// (FP64 only: it measured no faster in FP32).
+template <typename T, int TX, bool MASKED, bool KTX>
+pt_status launch_stream_tx_k(pt_op *op, const T *K, const T *u, T *y, int zb, int ze)
+{
+  if (MASKED && !op->d_mbits) return fail(PT_ERR_STATE, "masked apply without the packed Dirichlet bits");
+  if (KTX && op->MXP != TX) return fail(PT_ERR_STATE, "K row stride differs from the tile width");
+  constexpr size_t smem = ptk::stream_smem_bytes<T, TX>();
+  pt_status as = kernel_attrs((const void *)ptk::a11_stream_kernel<T, TX, MASKED, KTX>, smem);
+  if (as != PT_OK) return as;
+  const uint32_t *mb = MASKED ? op->d_mbits : nullptr;
+  return stream_colours<TX>(op, smem, zb, ze, [&](const cudaLaunchConfig_t &cfg, const ptk::StreamGrid &g) {
+    const cudaError_t e = cudaLaunchKernelEx(&cfg, ptk::a11_stream_kernel<T, TX, MASKED, KTX>, g, K, u, mb, y);
+    if (e != cudaSuccess) return fail(PT_ERR_CUDA, "streaming A11 launch: %s", cudaGetErrorString(e));
+    return PT_OK;
+  });
 }
 
 template <typename T, int TX, bool MASKED>
@@ -328,6 +342,29 @@ pt_status launch_stream_tx(pt_op *op, const T *K, const T *u, T *y, int zb = 0, 
     if (op->MXP == TX) return launch_stream_tx_k<T, TX, MASKED, true>(op, K, u, y, zb, ze);
   }
   return launch_stream_tx_k<T, TX, MASKED, false>(op, K, u, y, zb, ze);
+}
+
+// diag(A11) on the streaming tiles from the stored K (whole box, one launch
+// per colour class, programmatic like the apply).
+template <int TX, bool KTX>
+pt_status launch_diag_stream_tx(pt_op *op, double *d)
+{
+  constexpr size_t smem = ptk::diag_smem_bytes<TX>();
+  pt_status as = kernel_attrs((const void *)ptk::diag_stream_kernel<TX, KTX>, smem);
+  if (as != PT_OK) return as;
+  const double *K = op->d_K;
+  return stream_colours<TX>(op, smem, 0, -1, [&](const cudaLaunchConfig_t &cfg, const ptk::StreamGrid &g) {
+    const cudaError_t e = cudaLaunchKernelEx(&cfg, ptk::diag_stream_kernel<TX, KTX>, g, K, d);
+    if (e != cudaSuccess) return fail(PT_ERR_CUDA, "streaming diag launch: %s", cudaGetErrorString(e));
+    return PT_OK;
+  });
+}
+
+pt_status launch_diag_stream(pt_op *op, double *d)
+{
+  if (op->TX == 32) return op->MXP == 32 ? launch_diag_stream_tx<32, true>(op, d) : launch_diag_stream_tx<32, false>(op, d);
+  if (op->TX == 64) return op->MXP == 64 ? launch_diag_stream_tx<64, true>(op, d) : launch_diag_stream_tx<64, false>(op, d);
+  return op->MXP == 128 ? launch_diag_stream_tx<128, true>(op, d) : launch_diag_stream_tx<128, false>(op, d);
 }
 
 template <typename T, bool MASKED>
@@ -490,6 +527,14 @@ pt_status diag_d(pt_op *op, double *d)
       ptk::ebe_diag_kernel<<<grid_stride_blocks(op->nvel), 256, 0, op->stream>>>(op->box, op->d_Ae, d);
       PT_LAUNCHED(op);
       return PT_OK;
+    }
+  }
+  if (op->a11_kernel == A11_STREAM) {
+    // the streaming tiles from the stored K, as the apply
+    if ((s = ensure_geometry(op)) != PT_OK) return s;
+    if (op->geom_ok) {
+      if (!op->full_box) PT_CUDA(cudaMemsetAsync(d, 0, sizeof(double) * op->nvel, op->stream));
+      return launch_diag_stream(op, d);
     }
   }
   s = upload_diag_tables();

@@ -142,6 +142,114 @@ PT_HD void qp_action_K(const T Kq[9], T G[3][3][9], int p)
     for (int l = 0; l < 3; l++) G[k][l][p] = S[0][l] * Kq[k] + (S[1][l] * Kq[3 + k] + S[2][l] * Kq[6 + k]);
 }
 
+// ---------------------------------------------------------------------------
+// diag(A11) from K (the streaming diagonal kernel).
+//
+// For basis function n and velocity component m the A11 action above applied
+// to u = N_n e_m gives, at each point, A[k][l] = delta_lm a_k with
+//   a_k(n,q) = sum_d K[3k+d](q) g'_d(n,q),   g' = h^-1 grad_xi N_n,
+// and the diagonal entry sum_q sum_k (a_k + delta_km a_m) a_k, i.e.
+//   diag(n, m) = Q_m(n) + sum_k Q_k(n),   Q_k(n) = sum_q a_k(n,q)^2
+// (the reference's w det eta (|grad N|^2 + (dN/dx_m)^2) of
+// src/stokes_q2p1_mf_operators_diag_def.c:120-205 in K form).
+//
+// Q_k is a quadratic form in g': with r = row k of K at a point,
+//   a_k^2 = sum_{d,e} r_d r_e g'_d g'_e,
+// and g'_d g'_e factorises per axis: along axis t it is E(g,i)^2 if d = e = t,
+// E(g,i) B(g,i) if exactly one of d, e is t and B(g,i)^2 otherwise (B the Q2
+// basis and E = D/h its scaled derivative at Gauss abscissa g, node i).  So
+// the six products r_d r_e (cross terms doubled) of a Gauss plane are
+// contracted along xi, then along eta and summed by their zeta factor
+// (BB: de = 00, 11, 01; EB: 02, 12; EE: 22), and the zeta factors of the
+// plane spread the three sums over the node planes: ~400 operations per
+// plane and component instead of 27 x 9 x 4 for the point-by-node sum.
+// ---------------------------------------------------------------------------
+namespace dg {
+// B(g,i) and E(g,i) = D(g,i)/h (rows of q2::B* and the DZ constants above)
+PT_HD constexpr double xb(int g, int i)
+{
+  return g == 1 ? (i == 1 ? 1.0 : 0.0) : (i == 1 ? B1 : (((g == 0) == (i == 0)) ? B0 : B2));
+}
+PT_HD constexpr double xe(int g, int i)
+{
+  return g == 1 ? (i == 0 ? -GS : (i == 1 ? 0.0 : GS))
+                : (g == 0 ? (i == 0 ? DZ00 : (i == 1 ? DZ01 : DZ02)) : (i == 0 ? DZ20 : (i == 1 ? DZ21 : DZ22)));
+}
+PT_HD constexpr double bb(int g, int i) { return xb(g, i) * xb(g, i); }
+PT_HD constexpr double eb(int g, int i) { return xe(g, i) * xb(g, i); }
+PT_HD constexpr double ee(int g, int i) { return xe(g, i) * xe(g, i); }
+
+// acc += f c, skipped where the compile-time factor c is zero (the middle
+// Gauss point: B = [0 1 0], E = [-s 0 s], so EB = 0 there)
+template <typename T>
+PT_HD void cacc(T &acc, T f, double c)
+{
+  if (c != 0.0) acc += f * T(c);
+}
+}  // namespace dg
+
+// Q[k*9 + j*3 + i] = sum over the 9 points p = b*3 + c (b along eta, c along
+// xi) of one Gauss plane of a(n,p)^2 for node n = (i,j,k), a = r . g'.
+// kr(p, d) returns component d of the row of K at point p; z[s][k] are the
+// plane's zeta factors (s = 0: B^2, 1: E B, 2: E^2 at its Gauss abscissa).
+template <typename T, typename KR>
+PT_HD void diag_form_plane(KR kr, const T z[3][3], T Q[27])
+{
+  using namespace dg;
+  T Z[3][9];  // [BB, EB, EE][j*3+i]
+#pragma unroll
+  for (int b = 0; b < 3; b++) {
+    T X[6][3];  // products [00, 11, 22, 01, 02, 12] contracted along xi, [i]
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      const int p = 3 * b + c;
+      const T k0 = kr(p, 0), k1 = kr(p, 1), k2 = kr(p, 2);
+      const T t0 = k0 + k0, t1 = k1 + k1;
+      const T f00 = k0 * k0, f11 = k1 * k1, f22 = k2 * k2, f01 = t0 * k1, f02 = t0 * k2, f12 = t1 * k2;
+#pragma unroll
+      for (int i = 0; i < 3; i++) {
+        if (c == 0) {  // every factor of the first abscissa is non-zero
+          X[0][i] = f00 * T(ee(0, i));
+          X[1][i] = f11 * T(bb(0, i));
+          X[2][i] = f22 * T(bb(0, i));
+          X[3][i] = f01 * T(eb(0, i));
+          X[4][i] = f02 * T(eb(0, i));
+          X[5][i] = f12 * T(bb(0, i));
+        } else {
+          cacc(X[0][i], f00, ee(c, i));
+          cacc(X[1][i], f11, bb(c, i));
+          cacc(X[2][i], f22, bb(c, i));
+          cacc(X[3][i], f01, eb(c, i));
+          cacc(X[4][i], f02, eb(c, i));
+          cacc(X[5][i], f12, bb(c, i));
+        }
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < 3; j++)
+#pragma unroll
+      for (int i = 0; i < 3; i++) {
+        T &zbb = Z[0][3 * j + i], &zeb = Z[1][3 * j + i], &zee = Z[2][3 * j + i];
+        if (b == 0) {
+          zbb = X[0][i] * T(bb(0, j)) + (X[1][i] * T(ee(0, j)) + X[3][i] * T(eb(0, j)));
+          zeb = X[4][i] * T(bb(0, j)) + X[5][i] * T(eb(0, j));
+          zee = X[2][i] * T(bb(0, j));
+        } else {
+          cacc(zbb, X[0][i], bb(b, j));
+          cacc(zbb, X[1][i], ee(b, j));
+          cacc(zbb, X[3][i], eb(b, j));
+          cacc(zeb, X[4][i], bb(b, j));
+          cacc(zeb, X[5][i], eb(b, j));
+          cacc(zee, X[2][i], bb(b, j));
+        }
+      }
+  }
+#pragma unroll
+  for (int k = 0; k < 3; k++)
+#pragma unroll
+    for (int ji = 0; ji < 9; ji++) Q[9 * k + ji] = z[0][k] * Z[0][ji] + (z[1][k] * Z[1][ji] + z[2][k] * Z[2][ji]);
+}
+
 // K at one Gauss point from J (d x_l / d xi_d) and the weight*eta product.
 // Returns false when c = w eta / det is not positive and finite.
 template <typename T>

@@ -153,3 +153,56 @@ extern "C" int core_a11_plane_f32(int mx, int my, int mz, const double *coords, 
 {
   return a11_plane_mesh<float>(mx, my, mz, coords, eta, u, y);
 }
+
+// The streaming diagonal kernel's algorithm (q2::diag_form_plane): K per
+// Gauss point, then per quadrature plane and velocity component the
+// sum-factorised quadratic form Q_m; diag(n, l) = Q_l(n) + sum_m Q_m(n).
+extern "C" int core_diag_plane_f64(int mx, int my, int mz, const double *coords, const double *eta, double *y)
+{
+  const int64_t X = 2 * mx + 1, Y = 2 * my + 1;
+  int bad = 0;
+  double zf[3][3][3];  // [plane A][BB, EB, EE][k]
+  for (int a = 0; a < 3; a++)
+    for (int k = 0; k < 3; k++) {
+      zf[a][0][k] = q2::dg::bb(a, k);
+      zf[a][1][k] = q2::dg::eb(a, k);
+      zf[a][2][k] = q2::dg::ee(a, k);
+    }
+  for (int ek = 0; ek < mz; ek++)
+    for (int ej = 0; ej < my; ej++)
+      for (int ei = 0; ei < mx; ei++) {
+        const int64_t e = ei + (int64_t)mx * (ej + (int64_t)my * ek);
+        int64_t nid[27];
+        for (int a = 0; a < 3; a++)
+          for (int b = 0; b < 3; b++)
+            for (int c = 0; c < 3; c++)
+              nid[9 * a + 3 * b + c] = (2 * ei + c) + (2 * ej + b) * X + (2 * ek + a) * X * Y;
+        double xf[27], I[27], Jg[3][3][27];
+        for (int l = 0; l < 3; l++) {
+          for (int n = 0; n < 27; n++) xf[n] = coords[3 * nid[n] + l];
+          q2::interp(xf, I);
+          q2::grad_colloc(I, Jg[0][l], Jg[1][l], Jg[2][l]);
+        }
+        double K[27][9];
+        for (int q = 0; q < 27; q++) {
+          double J[3][3];
+          for (int k = 0; k < 3; k++)
+            for (int l = 0; l < 3; l++) J[k][l] = Jg[k][l][q];
+          if (!q2::geom_K(J, q2::weight(q) * eta[27 * e + q], K[q])) bad++;
+        }
+        for (int a = 0; a < 3; a++) {
+          double S[27] = {0};
+          for (int m = 0; m < 3; m++) {
+            double Q[27];
+            q2::diag_form_plane<double>([&](int p, int d) { return K[9 * a + p][3 * m + d]; }, zf[a], Q);
+            for (int n = 0; n < 27; n++) {
+              y[3 * nid[n] + m] += Q[n];
+              S[n] += Q[n];
+            }
+          }
+          for (int n = 0; n < 27; n++)
+            for (int l = 0; l < 3; l++) y[3 * nid[n] + l] += S[n];
+        }
+      }
+  return bad;
+}

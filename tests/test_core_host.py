@@ -64,3 +64,15 @@ def test_stream_geometry_flags_nonpositive_viscosity(core):
     y = np.zeros(m.nvel)
     u = M.uniform_vec(m.nvel, 4)
     assert core.core_a11_plane_f64(*m.dims, _p(m.coords), _p(eta), _p(u), _p(y)) == 1
+
+
+@pytest.mark.parametrize("workload", ["c0", "box:1,1,1", "box:3,2,4"])
+def test_stream_diag_algorithm_matches_oracle(core, ora, workload):
+    """Sum-factorised diagonal from the Gauss-point factor K (the streaming
+    diag kernel's per-plane arithmetic, q2::diag_form_plane)."""
+    m, eta, _ = M.problem(workload)
+    ref = ora.diag(m.dims, m.coords, eta)
+    d = np.zeros(m.nvel)
+    core.core_diag_plane_f64.argtypes = [ctypes.c_int] * 3 + [ctypes.POINTER(ctypes.c_double)] * 3
+    assert core.core_diag_plane_f64(*m.dims, _p(m.coords), _p(eta), _p(d)) == 0
+    assert relerr(d, ref) < 1e-13
