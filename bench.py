@@ -912,7 +912,8 @@ def main():
                     help="apply mode: skip the solve / batched / served legs of the default line")
     ap.add_argument("--leg-nreq", type=int, default=100, help="served leg of the default line: requests")
     ap.add_argument("--leg-ncal", type=int, default=32, help="served leg: capacity calibration requests")
-    ap.add_argument("--leg-nserial", type=int, default=8, help="served leg: requests solved one at a time")
+    ap.add_argument("--leg-nserial", type=int, default=100,
+                    help="served leg: requests solved one at a time (all of the leg's requests by default)")
     ap.add_argument("--ksp", default="fcg")
     ap.add_argument("--rtol", type=float, default=1e-8)
     ap.add_argument("--max-it", type=int, default=20000)

@@ -40,37 +40,6 @@ constexpr size_t diag_smem_bytes()
   return sizeof(double) * ((size_t)L::TILE + L::SIDE);
 }
 
-// Adds V (27 node values [k*9 + j*3 + i]) to component l of the thread's
-// nodes in the tile: node columns i = 0, 1, then (after the warp's other
-// lanes) i = 2, whose column lane 31 of every warp but the last keeps in the
-// side buffer -- the A11 kernel's order, so shared columns are summed in a
-// fixed order.
-template <int TX>
-__device__ __forceinline__ void diag_add_nodes(double *yt, double *side, const int sl[3], int t, int warp,
-                                               bool to_side, unsigned amask, int l, const double V[27])
-{
-  using L = TileLayout<TX>;
-#pragma unroll
-  for (int i = 0; i < 3; i++) {
-    if (i == 2) __syncwarp(amask);
-#pragma unroll
-    for (int j = 0; j < 3; j++) {
-      if (i == 2 && to_side) {
-        double *sb = side + warp * 27 + 3 * j + l;
-        sb[sl[0] * 9] += V[3 * j + i];
-        sb[sl[1] * 9] += V[9 + 3 * j + i];
-        sb[sl[2] * 9] += V[18 + 3 * j + i];
-      } else {
-        const int n = 2 * t + i;
-        yt[L::at(l, sl[0], j, n)] += V[3 * j + i];
-        yt[L::at(l, sl[1], j, n)] += V[9 + 3 * j + i];
-        yt[L::at(l, sl[2], j, n)] += V[18 + 3 * j + i];
-      }
-    }
-  }
-  __syncwarp(amask);
-}
-
 // One element (thread t), quadrature plane A: Q_m for m = 0..2 into the
 // tile, then S.  Ke points at K(row, q = 0, r = 0, ex).
 template <int TX, bool KTX>
@@ -98,10 +67,10 @@ __device__ __forceinline__ void diag_element_plane(int A, double *yt, double *si
 #pragma unroll
       for (int n = 0; n < 27; n++) S[n] += Q[n];
     }
-    diag_add_nodes<TX>(yt, side, sl, t, warp, to_side, amask, m, Q);
+    tile_add_nodes<double, TX>(yt, side, sl, t, warp, to_side, amask, m, Q);
   }
 #pragma unroll 1
-  for (int l = 0; l < 3; l++) diag_add_nodes<TX>(yt, side, sl, t, warp, to_side, amask, l, S);
+  for (int l = 0; l < 3; l++) tile_add_nodes<double, TX>(yt, side, sl, t, warp, to_side, amask, l, S);
 }
 
 // One tile (x-tile tx, row ej, z-chunk zc); the whole CTA.
@@ -158,10 +127,11 @@ __device__ __forceinline__ void diag_tile(const StreamGrid &g, int tx, int ej, i
 }
 
 // Resident CTAs per SM the register budget is sized for: 256 threads per SM
-// (~250 registers, no spill).  Measured at 128^3: 1.93 ms against 2.39 ms at
-// 384 threads per SM (168 registers, a small spill) and 2.53 ms for a form
-// without S in registers (Q_m added to all three components, 128 registers,
-// 384 threads per SM, three times the shared-memory adds).
+// (230 registers, no spill).  Measured at 128^3 with the batched tile adds:
+// 1.44 ms against 1.63 ms at 384 threads per SM (168 registers, a small
+// spill); before the adds were batched, 1.93 ms against 2.39 ms, and 2.53 ms
+// for a form without S in registers (Q_m added to all three components, 128
+// registers, 384 threads per SM, three times the shared-memory adds).
 template <int TX>
 constexpr int diag_min_blocks()
 {

@@ -307,6 +307,54 @@ __device__ __forceinline__ void zeta_bwd_rt(int A, T q, T r, T &c0, T &c1, T &c2
   c2 = T(c_zB[A][2]) * q + T(c_zD[A][2]) * r;
 }
 
+// Adds V (27 node values [k*9 + j*3 + i]) to component l of thread t's nodes
+// in the tile: node columns i = 0, 1, then (after the warp's other lanes)
+// i = 2, whose column lane 31 of every warp but the last keeps in the side
+// buffer, so a column shared by two elements is summed in a fixed order.
+// Each group's entries are all read before any is written: the slots are
+// runtime indices, so the compiler cannot tell the 18 (9) addresses apart and
+// would otherwise wait out a shared-memory round trip per entry.
+template <typename T, int TX>
+__device__ __forceinline__ void tile_add_nodes(T *yt, T *side, const int sl[3], int t, int warp, bool to_side,
+                                               unsigned amask, int l, const T V[27])
+{
+  using L = TileLayout<TX>;
+  {
+    T *b0 = yt + L::at(l, 0, 0, 2 * t), *b1 = yt + L::at(l, 0, 0, 2 * t + 1);
+    T c[18];
+#pragma unroll
+    for (int k = 0; k < 3; k++)
+#pragma unroll
+      for (int j = 0; j < 3; j++) {
+        c[6 * k + 2 * j] = b0[sl[k] * L::PLANE + j * L::ROW];
+        c[6 * k + 2 * j + 1] = b1[sl[k] * L::PLANE + j * L::ROW];
+      }
+#pragma unroll
+    for (int k = 0; k < 3; k++)
+#pragma unroll
+      for (int j = 0; j < 3; j++) {
+        b0[sl[k] * L::PLANE + j * L::ROW] = c[6 * k + 2 * j] + V[9 * k + 3 * j];
+        b1[sl[k] * L::PLANE + j * L::ROW] = c[6 * k + 2 * j + 1] + V[9 * k + 3 * j + 1];
+      }
+  }
+  __syncwarp(amask);
+  {
+    // column i = 2: the next lane's i = 0 column, or the side buffer
+    T *b2 = to_side ? side + warp * 27 + l : yt + L::at(l, 0, 0, 2 * t + 2);
+    const int ss = to_side ? 9 : L::PLANE, rs = to_side ? 3 : L::ROW;
+    T c[9];
+#pragma unroll
+    for (int k = 0; k < 3; k++)
+#pragma unroll
+      for (int j = 0; j < 3; j++) c[3 * k + j] = b2[sl[k] * ss + j * rs];
+#pragma unroll
+    for (int k = 0; k < 3; k++)
+#pragma unroll
+      for (int j = 0; j < 3; j++) b2[sl[k] * ss + j * rs] = c[3 * k + j] + V[9 * k + 3 * j + 2];
+  }
+  __syncwarp(amask);
+}
+
 // One element (thread t of the tile), quadrature plane A: forward from the u
 // tile, viscous action with K, transpose accumulated into the y tile.  KTX:
 // the K rows are one tile wide (MXP == TX), a compile-time stride whose
@@ -368,27 +416,10 @@ __device__ __forceinline__ void element_plane(int A, const T *ut, T *yt, T *side
   for (int l = 0; l < 3; l++) {
     T Qt[9], Rt[9];
     q2::plane_bwd(G[0][l], G[1][l], G[2][l], Qt, Rt);
+    T C[27];  // [k*9 + j*3 + i]
 #pragma unroll
-    for (int i = 0; i < 3; i++) {
-      if (i == 2) __syncwarp(amask);
-#pragma unroll
-      for (int j = 0; j < 3; j++) {
-        T c0, c1, c2;
-        zeta_bwd_rt<T>(A, Qt[3 * j + i], Rt[3 * j + i], c0, c1, c2);
-        if (i == 2 && to_side) {
-          T *sb = side + warp * 27 + 3 * j + l;
-          sb[sl[0] * 9] += c0;
-          sb[sl[1] * 9] += c1;
-          sb[sl[2] * 9] += c2;
-        } else {
-          const int n = 2 * t + i;
-          yt[L::at(l, sl[0], j, n)] += c0;
-          yt[L::at(l, sl[1], j, n)] += c1;
-          yt[L::at(l, sl[2], j, n)] += c2;
-        }
-      }
-    }
-    __syncwarp(amask);
+    for (int ji = 0; ji < 9; ji++) zeta_bwd_rt<T>(A, Qt[ji], Rt[ji], C[ji], C[9 + ji], C[18 + ji]);
+    tile_add_nodes<T, TX>(yt, side, sl, t, warp, to_side, amask, l, C);
   }
 }
 
