@@ -92,6 +92,27 @@ def test_apply_is_deterministic(torch_cuda):
         assert torch.equal(y1, y2)
 
 
+def test_stream_diag_runs_on_the_streaming_tiles(torch_cuda, ora):
+    """diag(A11) of a streaming op is the sum-factorised kernel on the
+    streaming tiles: one launch per colour class of tiles (4 for a box one
+    tile wide), not the 8-colour element kernel; bitwise repeatable, and
+    equal to the oracle and to the 8-colour kernel to FP64 rounding."""
+    torch = torch_cuda
+    m, eta, _ = M.problem("box:17,9,6", seed=6)
+    with make_op(m, eta, None, "b200_stream") as a, make_op(m, eta, None, "b200_colour") as b:
+        d1 = a.MFStokesWrapper_diagA11(torch.empty(m.nvel, dtype=torch.float64, device="cuda")).clone()
+        a.reset_launch_count()
+        d2 = a.MFStokesWrapper_diagA11(torch.empty(m.nvel, dtype=torch.float64, device="cuda"))
+        torch.cuda.synchronize()
+        assert a.launch_count() == 4
+        assert torch.equal(d1, d2)
+        dc = b.MFStokesWrapper_diagA11(torch.empty(m.nvel, dtype=torch.float64, device="cuda"))
+        torch.cuda.synchronize()
+        d = d2.cpu().numpy()
+        assert relerr(d, ora.diag(m.dims, m.coords, eta)) < TOL64
+        assert relerr(d, dc.cpu().numpy()) < 1e-14
+
+
 @pytest.mark.parametrize("other", ["b200_colour", "b200_ebe"])
 @pytest.mark.parametrize("workload", ["box:40,7,5", "box:150,3,9", "box:128,4,6"])
 def test_kernels_agree(torch_cuda, workload, other):
