@@ -59,7 +59,7 @@ __device__ __forceinline__ void diag_element_plane(int A, double *yt, double *si
   for (int m = 0; m < 3; m++) {
     const double *km = kp + (int64_t)(3 * m) * MXP;
     double Q[27];
-    q2::diag_form_plane<double>([&](int p, int d) { return km[(int64_t)(9 * p + d) * MXP]; }, z, Q);
+    q2::diag_form_plane<double>([&](int p, int d) { return ldk(km + (int64_t)(9 * p + d) * MXP); }, z, Q);
     if (m == 0) {
 #pragma unroll
       for (int n = 0; n < 27; n++) S[n] = Q[n];
