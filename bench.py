@@ -56,8 +56,8 @@ WORKLOAD_TEXT = {
 }
 # DRAM bytes per element of one FP64 streaming apply (K 1.94 KB + u/y tiles),
 # measured with ncu on a 128x128x32 box (rows of 128 elements): 2 colour
-# launches averaged 0.327 GB read + 0.032 GB written for 128*128*32/4 elements.
-TRAFFIC_PER_ELEMENT_F64 = 4 * (0.327e9 + 0.032e9) / (128 * 128 * 32)
+# launches averaged 0.3195 GB read + 0.0184 GB written for 128*128*32/4 elements.
+TRAFFIC_PER_ELEMENT_F64 = 4 * (0.3195e9 + 0.0184e9) / (128 * 128 * 32)
 UNIT = "GDoF/s"
 
 
